@@ -1,0 +1,102 @@
+// Internal interface between the C ABI layer (capi.cu) and the kernel files.
+// Every launcher enqueues on `st` and returns a cudaError_t (cudaSuccess when
+// the launch was accepted); it never synchronises.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+#include <cuda_runtime.h>
+
+#include "vb_common.cuh"
+
+namespace vb {
+
+enum Depth : int { k8U = 0, k16U = 2, k16S = 3, k32F = 5 };
+
+inline int depth_size(int d) { return d == k8U ? 1 : (d == k16U || d == k16S) ? 2 : d == k32F ? 4 : 0; }
+
+// Counts kernel launches made by the library (reported by visar_cuda_launch_count).
+void note_launch(int n = 1);
+
+// ------------------------------------------------------------- color
+// Conversion kinds of src/imgproc/color.zig:44-46.
+enum ColorKind : int { kReorder, kGray, kFromGray, kHsv, kFromHsv, kYcrcb, kFromYcrcb };
+struct ColorInfo {
+  int scn, dcn, sb, db;
+  ColorKind kind;
+};
+cudaError_t launch_cvt_color(const DImg &s, const DImg &d, int depth, const ColorInfo &ci, cudaStream_t st);
+
+// ---------------------------------------------------- separable filter
+// Finishing step of a separable filter (src/imgproc/filter.zig:60-116).
+enum Finish : int {
+  kFinShift,   // (v + 2^(s-1)) >> s, clamped to D's maximum (u8 / u16 fixed point)
+  kFinCast,    // saturating cast (satV)
+  kFinScaled,  // f32(v) * f32(scale), saturating cast
+};
+// Accumulator kinds: exact integers, or f32 in VISAR's operation order.
+enum Acc : int { kAccI32, kAccI64, kAccF32 };
+
+struct SepSpec {
+  int sdepth, ddepth;
+  Acc acc;
+  Finish fin;
+  int shift;      // kFinShift
+  double scale;   // kFinScaled
+  std::vector<int> kxi, kyi;    // integer taps (kAccI32 / kAccI64)
+  std::vector<float> kxf, kyf;  // f32 taps (kAccF32)
+  int border;
+};
+cudaError_t launch_sep_filter(const DImg &s, const DImg &d, const SepSpec &spec, cudaStream_t st);
+
+// ----------------------------------------------------------- resize
+struct LinTap { int o0, o1, w0, w1; };            // u8 bilinear tap (offsets in pixels or rows)
+struct CubTap { int o[4]; int w[4]; };            // u8 bicubic tap
+struct FLinTap { int o0, o1; float a0, a1; };      // generic bilinear
+struct FCubTap { int o[4]; float w[4]; };          // generic bicubic
+struct AreaEnt { int di, si; float alpha; };       // INTER_AREA table entry
+
+cudaError_t launch_resize_nearest(const DImg &s, const DImg &d, int depth, const int *xofs_dev, const int *yofs_dev, cudaStream_t st);
+cudaError_t launch_resize_u8_linear(const DImg &s, const DImg &d, const LinTap *xt, const LinTap *yt, cudaStream_t st);
+cudaError_t launch_resize_u8_half(const DImg &s, const DImg &d, cudaStream_t st);
+cudaError_t launch_resize_u8_cubic(const DImg &s, const DImg &d, const CubTap *xt, const CubTap *yt, cudaStream_t st);
+cudaError_t launch_resize_area_int(const DImg &s, const DImg &d, int depth, int ix, int iy, bool u8fast, cudaStream_t st);
+cudaError_t launch_resize_area_frac(const DImg &s, const DImg &d, int depth, const AreaEnt *xtab, int nx,
+                                    const int *xstart, const AreaEnt *ytab, const int *ystart, cudaStream_t st);
+cudaError_t launch_resize_linear_generic(const DImg &s, const DImg &d, int depth, const FLinTap *xt, const FLinTap *yt, cudaStream_t st);
+cudaError_t launch_resize_cubic_generic(const DImg &s, const DImg &d, int depth, const FCubTap *xt, const FCubTap *yt, cudaStream_t st);
+cudaError_t launch_copy_image(const DImg &s, const DImg &d, int depth, cudaStream_t st);
+
+// -------------------------------------------------------------- warps
+cudaError_t launch_warp_affine(const DImg &s, const DImg &d, int depth, const float m[6], int interp, int border,
+                               double value, cudaStream_t st);
+cudaError_t launch_warp_perspective(const DImg &s, const DImg &d, int depth, const double m[9], int interp, int border,
+                                    double value, cudaStream_t st);
+
+// ---------------------------------------------------------- threshold
+// Applies a fixed threshold. For u8 the LUT decides (covers every type and
+// out-of-range threshold); other depths compare.
+cudaError_t launch_threshold_lut_u8(const DImg &s, const DImg &d, const uint8_t *lut_dev, cudaStream_t st);
+cudaError_t launch_threshold_cmp(const DImg &s, const DImg &d, int depth, int type, double t, double m, cudaStream_t st);
+// Auto threshold (Otsu / triangle) of a u8 one-channel image: histogram, then
+// the f64 scan on the device; the chosen threshold is written to *thresh_dev
+// and the u8 LUT of `type` to lut_dev.
+cudaError_t launch_threshold_auto_u8(const DImg &s, int method, int type, double maxval, uint32_t *hist_dev,
+                                     double *thresh_dev, uint8_t *lut_dev, cudaStream_t st);
+cudaError_t launch_fill(const DImg &d, int depth, double value, cudaStream_t st);
+
+// -------------------------------------------------------- morphology
+struct MorphRun { int ky, x0, len; };
+cudaError_t launch_morph_pass(const DImg &s, const DImg &d, int depth, bool is_max, int kw, int kh, int ax, int ay,
+                              const MorphRun *runs_dev, int nruns, bool rect, cudaStream_t st);
+cudaError_t launch_sub_sat(const DImg &a, const DImg &b, const DImg &d, int depth, cudaStream_t st);
+
+// ------------------------------------------------------- host helpers
+// Gaussian taps (src/imgproc/filter.zig:350-476), in host f64.
+void gaussian_kernel(double *out, int n, double sigma);
+int gaussian_ksize(double sigma, bool depth_is_u8);
+void gaussian_kernel_fixed(int64_t *out, int n, double sigma, int bits);
+// getDerivKernels (src/imgproc/filter.zig:817-854). Returns false for an invalid kernel.
+bool deriv_kernel(int *out, int n, int order, int ksize);
+
+}  // namespace vb

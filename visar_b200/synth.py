@@ -1,0 +1,82 @@
+"""Seeded synthetic images with the shapes and value distributions of the
+benchmark workloads (VISAR publishes no dataset for this path).
+
+base_image: a horizontal gradient 0..255 across the width (same in every
+channel) plus uniform integer noise in [-20, 20], clamped to 0..255, with
+filled axis-aligned rectangles of random colour, 20-160 px per side.
+"""
+import numpy as np
+
+
+def base_image(h, w, c=3, nrect=8, seed=0, dtype=np.uint8):
+    rng = np.random.default_rng(seed)
+    x = np.arange(w, dtype=np.float64)
+    grad = np.rint(x * 255.0 / max(w - 1, 1)).astype(np.int32)
+    noise = rng.integers(-20, 21, size=(h, w, c), dtype=np.int32)
+    img = np.clip(grad[None, :, None] + noise, 0, 255).astype(np.uint8)
+    for _ in range(nrect):
+        rw = int(rng.integers(20, 161))
+        rh = int(rng.integers(20, 161))
+        x0 = int(rng.integers(0, max(1, w - rw + 1)))
+        y0 = int(rng.integers(0, max(1, h - rh + 1)))
+        col = rng.integers(0, 256, size=c, dtype=np.int32).astype(np.uint8)
+        img[y0:y0 + rh, x0:x0 + rw] = col
+    if c == 1:
+        img = img[:, :, 0]
+    if dtype == np.uint8:
+        return np.ascontiguousarray(img)
+    if dtype == np.uint16:
+        return img.astype(np.uint16) * 257
+    if dtype == np.int16:
+        return img.astype(np.int16) - 128
+    if dtype == np.float32:
+        return img.astype(np.float32) / 255.0
+    raise ValueError(dtype)
+
+
+def normal_f32(h, w, c=1, seed=0):
+    """float32 N(0, 1) samples (the f32 Gaussian workload)."""
+    rng = np.random.default_rng(seed)
+    shape = (h, w) if c == 1 else (h, w, c)
+    return rng.standard_normal(shape, dtype=np.float32)
+
+
+def rotation_matrix_2d(cx, cy, angle_deg, scale):
+    """OpenCV's getRotationMatrix2D (angle in degrees, counter-clockwise)."""
+    a = angle_deg * np.pi / 180.0
+    alpha = np.cos(a) * scale
+    beta = np.sin(a) * scale
+    return np.array([[alpha, beta, (1 - alpha) * cx - beta * cy],
+                     [-beta, alpha, beta * cx + (1 - alpha) * cy]], np.float64)
+
+
+def affine_params(w, h, seed):
+    """A seeded rotation +-30 deg, scale 0.8-1.2 about the centre, plus +-50 px translation."""
+    rng = np.random.default_rng(seed)
+    ang = rng.uniform(-30, 30)
+    sc = rng.uniform(0.8, 1.2)
+    m = rotation_matrix_2d(w / 2.0, h / 2.0, ang, sc)
+    m[0, 2] += rng.uniform(-50, 50)
+    m[1, 2] += rng.uniform(-50, 50)
+    return m
+
+
+def homography_from_corners(src_pts, dst_pts):
+    """The 3x3 homography mapping 4 source corners to 4 destination corners (f64 DLT solve)."""
+    a = []
+    b = []
+    for (x, y), (u, v) in zip(src_pts, dst_pts):
+        a.append([x, y, 1, 0, 0, 0, -u * x, -u * y])
+        b.append(u)
+        a.append([0, 0, 0, x, y, 1, -v * x, -v * y])
+        b.append(v)
+    h = np.linalg.solve(np.array(a, np.float64), np.array(b, np.float64))
+    return np.append(h, 1.0).reshape(3, 3)
+
+
+def perspective_params(w, h, seed, jitter=80.0):
+    """Each image corner jittered uniformly by +-jitter px; the homography from the jittered corners."""
+    rng = np.random.default_rng(seed)
+    src = [(0.0, 0.0), (w - 1.0, 0.0), (w - 1.0, h - 1.0), (0.0, h - 1.0)]
+    dst = [(x + rng.uniform(-jitter, jitter), y + rng.uniform(-jitter, jitter)) for x, y in src]
+    return homography_from_corners(src, dst)
