@@ -242,7 +242,11 @@ def main():
         torch.cuda.set_device(0)
     import visar_b200 as vb
     dev = torch.cuda.current_device()
-    stream = torch.cuda.current_stream()
+    # A real stream (torch's default stream has a NULL handle, which the
+    # library reads as "use your own stream"): events, the L2 flush and the
+    # library's kernels are all ordered on it.
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     vb.set_stream(stream)
 
     img, f, maff, mper = make_inputs()

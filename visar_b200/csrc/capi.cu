@@ -55,8 +55,13 @@ void ck(cudaError_t e) {
   fail(VISAR_INTERNAL, buf);
 }
 
+// The device of the current call: the one owning its device-resident
+// images (set while validating them), else the thread's current device.
+thread_local int t_hint_dev = -1;
+
 template <class F>
 int guarded(F &&f) {
+  t_hint_dev = -1;
   try {
     f();
     return VISAR_OK;
@@ -102,8 +107,13 @@ struct Call {
 
 Call begin_call() {
   int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) ck(e);
+  if (t_hint_dev >= 0) {
+    ck(cudaSetDevice(t_hint_dev));
+    dev = t_hint_dev;
+  } else {
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) ck(e);
+  }
   if (dev < 0 || dev >= 64) fail(VISAR_INTERNAL, "CudaError: device index");
   DevCtx &c = g_ctx[dev];
   if (!c.init) {
@@ -158,7 +168,12 @@ bool is_device_ptr(const void *p) {
     cudaGetLastError();
     return false;
   }
-  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+  const bool dev = a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+  if (dev && a.device >= 0) {
+    if (t_hint_dev >= 0 && t_hint_dev != a.device) fail(VISAR_INVALID_ARGUMENT, "InvalidArgument");
+    t_hint_dev = a.device;
+  }
+  return dev;
 }
 
 // typed(T, c): the checks of src/capi.zig:123-132 and Image.fromSliceStrided
@@ -784,7 +799,13 @@ int visar_sobel(const visar_image *src, const visar_image *dst, int dx, int dy, 
       for (int v : kx) sp.kxf.push_back((float)v);
       for (int v : ky) sp.kyf.push_back((float)v);
     } else {
-      sp.acc = kAccI32;
+      // VISAR sums in i16 or i32 (filter.zig:886-905); where 255 * sum|kx| *
+      // sum|ky| exceeds i32 (large apertures) its sums overflow, which Zig
+      // leaves undefined. The exact sum is kept in 64 bits there.
+      long long bx = 0, by = 0;
+      for (int v : kx) bx += v < 0 ? -v : v;
+      for (int v : ky) by += v < 0 ? -v : v;
+      sp.acc = (255.0 * (double)bx * (double)by > 2147483647.0) ? kAccI64 : kAccI32;
       sp.kxi = kx;
       sp.kyi = ky;
       sp.fin = scale == 1.0 ? kFinCast : kFinScaled;

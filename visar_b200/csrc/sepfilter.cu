@@ -306,6 +306,10 @@ cudaError_t launch_sep_filter(const DImg &s, const DImg &d, const SepSpec &sp, c
   }
   if (sp.sdepth == k16S && sp.ddepth == k16S && sp.fin == kFinScaled)
     return run<int16_t, int16_t, long long, int, kFinScaled>(s, d, a, st);
+  if (sp.sdepth == k8U && sp.ddepth == k16S) {
+    if (sp.fin == kFinCast) return run<uint8_t, int16_t, long long, int, kFinCast>(s, d, a, st);
+    if (sp.fin == kFinScaled) return run<uint8_t, int16_t, long long, int, kFinScaled>(s, d, a, st);
+  }
   return cudaErrorInvalidValue;
 }
 
