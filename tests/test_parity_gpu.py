@@ -355,3 +355,44 @@ def test_error_codes_match_oracle():
         with pytest.raises(O.OracleError) as e2:
             f(O)
         assert (e1.value.status, e1.value.name) == (e2.value.status, e2.value.name), f"case {i}"
+
+
+# ------------------------------------------------- fast-path coverage
+
+@pytest.mark.parametrize("cn", [1, 4])
+@pytest.mark.parametrize("h,w", [(37, 53), (64, 130), (1, 9), (9, 1), (200, 257)])
+def test_morphology_fast_shapes(cn, h, w):
+    a = natural(h, w, cn)
+    for shape in (0, 1, 2):
+        for kw, kh in [(3, 3), (5, 5), (7, 7), (9, 9), (3, 5), (5, 3), (9, 3), (1, 7), (7, 1)]:
+            for op in (0, 1, 2, 3):
+                _both(vb.morphology, O.morphology, a, op, shape, (kw, kh), what=f"morph c{cn} op{op} sh{shape} {kw}x{kh}")
+
+
+@pytest.mark.parametrize("cn", [1, 3, 4])
+@pytest.mark.parametrize("h,w", [(33, 67), (8, 5), (130, 509)])
+def test_fast_filters_odd_widths(cn, h, w):
+    for dt in (np.uint8, np.float32):
+        a = natural(h, w, cn, dt)
+        for k in (3, 5, 7):
+            for border in (0, 1, 2, 4):
+                _both(vb.gaussian_blur, O.gaussian_blur, a, (k, k), 0, 0, border, exact_f32=True,
+                      what=f"gauss fast {dt} c{cn} k{k} b{border} {w}x{h}")
+
+
+def test_fast_paths_unaligned_views_fall_back():
+    big = natural(90, 131, 1)
+    v = big[3:80, 1:120]  # row starts not 4-byte aligned
+    _both(vb.gaussian_blur, O.gaussian_blur, np.ascontiguousarray(v), (5, 5), 0, what="contig")
+    _both(vb.gaussian_blur, O.gaussian_blur, v, (5, 5), 0, what="unaligned view")
+    _both(vb.morphology, O.morphology, v, 2, 2, (5, 5), what="unaligned morph")
+    _both(vb.resize, O.resize, v, (59, 38), 1, what="unaligned resize")
+
+
+@pytest.mark.parametrize("cn", [1, 2, 3, 4])
+def test_resize_half_and_linear_vector_paths(cn):
+    for h, w in [(64, 128), (62, 130), (2, 8), (10, 18), (1081, 1921)]:
+        a = natural(h, w, cn)
+        _both(vb.resize, O.resize, a, (w // 2, h // 2), 1, what=f"half c{cn} {w}x{h}")
+        _both(vb.resize, O.resize, a, (w // 2, h // 2), 3, what=f"area half c{cn} {w}x{h}")
+        _both(vb.resize, O.resize, a, (max(1, w * 2 // 3), max(1, h * 2 // 3)), 1, what=f"lin c{cn} {w}x{h}")

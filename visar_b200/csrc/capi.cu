@@ -972,7 +972,11 @@ int visar_morphology(const visar_image *src, const visar_image *dst, int op, int
           else idv = is_max ? (depth == k16S ? -32768 : 0) : (depth == k8U ? 255 : depth == k16U ? 65535 : 32767);
           ck(launch_fill(out, depth, idv, call.st));
         } else {
-          ck(launch_morph_pass(cur, out, depth, is_max, kw, kh, ax, ay, runs_dev, (int)runs.size(), rect, call.st));
+          cudaError_t e = cudaErrorNotSupported;
+          if (depth == k8U) e = launch_morph_fast(cur, out, is_max, mask, kw, kh, call.st);
+          if (e == cudaErrorNotSupported)
+            e = launch_morph_pass(cur, out, depth, is_max, kw, kh, ax, ay, runs_dev, (int)runs.size(), rect, call.st);
+          ck(e);
         }
         cur = out;
       }

@@ -38,6 +38,68 @@ __global__ void __launch_bounds__(256) k_u8_linear(DImg s, DImg d, const LinTap 
   row_ptr<uint8_t>(d, y)[i] = (uint8_t)min(max((t + 2) >> 2, 0), 255);
 }
 
+// The same per output pixel with the channel count known at compile time:
+// one 16-byte tap load, 32-bit offsets, the row taps uniform per CTA row.
+template <int CN>
+__global__ void __launch_bounds__(256) k_u8_linear_c(DImg s, DImg d, const LinTap *xt, const LinTap *yt) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (x >= d.w) return;
+  const int4 tx = *reinterpret_cast<const int4 *>(xt + x);
+  const LinTap ty = yt[y];
+  const uint8_t *r0 = row_ptr<const uint8_t>(s, ty.o0);
+  const uint8_t *r1 = row_ptr<const uint8_t>(s, ty.o1);
+  const int a0 = tx.x * CN, a1 = tx.y * CN;
+  uint8_t *o = row_ptr<uint8_t>(d, y) + x * CN;
+#pragma unroll
+  for (int c = 0; c < CN; c++) {
+    const int h0 = ((int)r0[a0 + c] * tx.z + (int)r0[a1 + c] * tx.w) >> 4;
+    const int h1 = ((int)r1[a0 + c] * tx.z + (int)r1[a1 + c] * tx.w) >> 4;
+    const int t = ((h0 * ty.w0) >> 16) + ((h1 * ty.w1) >> 16);
+    o[c] = (uint8_t)min(max((t + 2) >> 2, 0), 255);
+  }
+}
+
+// Exact halving, 4 output pixels per thread through 8-byte loads and 4-byte
+// stores (rows 8-byte aligned; checked by the launcher).
+template <int CN>
+__global__ void __launch_bounds__(256) k_u8_half_v(DImg s, DImg d) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;  // group of 4 output pixels
+  const int y = blockIdx.y;
+  const int x0 = g * 4;
+  if (x0 >= d.w) return;
+  const uint8_t *a = row_ptr<const uint8_t>(s, 2 * y);
+  const uint8_t *b = row_ptr<const uint8_t>(s, 2 * y + 1);
+  uint8_t *o = row_ptr<uint8_t>(d, y);
+  if (x0 + 4 <= d.w) {
+    uint64_t ra[CN], rb[CN];
+#pragma unroll
+    for (int k = 0; k < CN; k++) {
+      ra[k] = reinterpret_cast<const uint64_t *>(a + (size_t)x0 * 2 * CN)[k];
+      rb[k] = reinterpret_cast<const uint64_t *>(b + (size_t)x0 * 2 * CN)[k];
+    }
+    const uint8_t *ba = reinterpret_cast<const uint8_t *>(ra);
+    const uint8_t *bb = reinterpret_cast<const uint8_t *>(rb);
+    uint32_t out[CN];
+    uint8_t *ob = reinterpret_cast<uint8_t *>(out);
+#pragma unroll
+    for (int p = 0; p < 4; p++)
+#pragma unroll
+      for (int c = 0; c < CN; c++) {
+        const int i = 2 * p * CN + c;
+        ob[p * CN + c] = (uint8_t)(((unsigned)ba[i] + ba[i + CN] + bb[i] + bb[i + CN] + 2) >> 2);
+      }
+#pragma unroll
+    for (int k = 0; k < CN; k++) reinterpret_cast<uint32_t *>(o + (size_t)x0 * CN)[k] = out[k];
+  } else {
+    for (int x = x0; x < d.w; x++)
+      for (int c = 0; c < CN; c++) {
+        const int i = 2 * x * CN + c;
+        o[x * CN + c] = (uint8_t)(((unsigned)a[i] + a[i + CN] + b[i] + b[i + CN] + 2) >> 2);
+      }
+  }
+}
+
 // Exact halving (resize_u8.zig:381-447): (a + b + c + d + 2) >> 2.
 __global__ void __launch_bounds__(256) k_u8_half(DImg s, DImg d) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -230,11 +292,29 @@ cudaError_t launch_resize_nearest(const DImg &s, const DImg &d, int depth, const
 
 cudaError_t launch_resize_u8_linear(const DImg &s, const DImg &d, const LinTap *xt, const LinTap *yt, cudaStream_t st) {
   if (d.w == 0 || d.h == 0) return cudaSuccess;
-  VB_LAUNCH(k_u8_linear, s, d, xt, yt);
+  const dim3 g(ceil_div(d.w, 256), d.h);
+  switch (d.cn) {
+    case 1: k_u8_linear_c<1><<<g, 256, 0, st>>>(s, d, xt, yt); break;
+    case 3: k_u8_linear_c<3><<<g, 256, 0, st>>>(s, d, xt, yt); break;
+    case 4: k_u8_linear_c<4><<<g, 256, 0, st>>>(s, d, xt, yt); break;
+    default: VB_LAUNCH(k_u8_linear, s, d, xt, yt);
+  }
+  note_launch();
+  return cudaGetLastError();
 }
 
 cudaError_t launch_resize_u8_half(const DImg &s, const DImg &d, cudaStream_t st) {
   if (d.w == 0 || d.h == 0) return cudaSuccess;
+  const bool al = ((uintptr_t)s.p % 8 == 0) && (s.stride % 8 == 0) && ((uintptr_t)d.p % 4 == 0) && (d.stride % 4 == 0);
+  const dim3 g(ceil_div(ceil_div(d.w, 4), 256), d.h);
+  if (al) {
+    switch (d.cn) {
+      case 1: k_u8_half_v<1><<<g, 256, 0, st>>>(s, d); note_launch(); return cudaGetLastError();
+      case 2: k_u8_half_v<2><<<g, 256, 0, st>>>(s, d); note_launch(); return cudaGetLastError();
+      case 3: k_u8_half_v<3><<<g, 256, 0, st>>>(s, d); note_launch(); return cudaGetLastError();
+      case 4: k_u8_half_v<4><<<g, 256, 0, st>>>(s, d); note_launch(); return cudaGetLastError();
+    }
+  }
   VB_LAUNCH(k_u8_half, s, d);
 }
 

@@ -261,6 +261,10 @@ cudaError_t run_float_cast_d(const DImg &s, const DImg &d, int ddepth, const Sep
 
 cudaError_t launch_sep_filter(const DImg &s, const DImg &d, const SepSpec &sp, cudaStream_t st) {
   if (s.w == 0 || s.h == 0) return cudaSuccess;
+  {
+    const cudaError_t e = launch_sep_fast(s, d, sp, 0, st);
+    if (e != cudaErrorNotSupported) return e;
+  }
   if (sp.acc == kAccF32) {
     if ((int)sp.kxf.size() > kMaxTaps || (int)sp.kyf.size() > kMaxTaps) return cudaErrorInvalidValue;
     const SepArgs<float> a = make_args<float>(s, sp.kxf, sp.kyf, sp, false);

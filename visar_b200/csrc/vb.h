@@ -48,9 +48,13 @@ struct SepSpec {
   int border;
 };
 cudaError_t launch_sep_filter(const DImg &s, const DImg &d, const SepSpec &spec, cudaStream_t st);
+// Register-window kernel for 3x3/5x5/7x7 u8 fixed-point and f32 filters on
+// 1/3/4 channels; cudaErrorNotSupported for any other shape. rows_hint <= 0
+// picks the row-band height from the image size.
+cudaError_t launch_sep_fast(const DImg &s, const DImg &d, const SepSpec &spec, int rows_hint, cudaStream_t st);
 
 // ----------------------------------------------------------- resize
-struct LinTap { int o0, o1, w0, w1; };            // u8 bilinear tap (offsets in pixels or rows)
+struct alignas(16) LinTap { int o0, o1, w0, w1; };  // u8 bilinear tap (offsets in pixels or rows)
 struct CubTap { int o[4]; int w[4]; };            // u8 bicubic tap
 struct FLinTap { int o0, o1; float a0, a1; };      // generic bilinear
 struct FCubTap { int o[4]; float w[4]; };          // generic bicubic
@@ -90,6 +94,10 @@ struct MorphRun { int ky, x0, len; };
 cudaError_t launch_morph_pass(const DImg &s, const DImg &d, int depth, bool is_max, int kw, int kh, int ax, int ay,
                               const MorphRun *runs_dev, int nruns, bool rect, cudaStream_t st);
 cudaError_t launch_sub_sat(const DImg &a, const DImg &b, const DImg &d, int depth, cudaStream_t st);
+// u8 pass for centred-run elements with a horizontal reach <= 4 samples;
+// cudaErrorNotSupported otherwise.
+cudaError_t launch_morph_fast(const DImg &s, const DImg &d, bool is_max, const std::vector<uint8_t> &mask, int kw, int kh,
+                              cudaStream_t st);
 
 // ------------------------------------------------------- host helpers
 // Gaussian taps (src/imgproc/filter.zig:350-476), in host f64.

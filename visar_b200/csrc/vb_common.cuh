@@ -34,6 +34,20 @@ __host__ __device__ __forceinline__ T *row_ptr(const DImg &im, long long y) {
 // a constant border outside the range.
 __host__ __device__ __forceinline__ int border_map(long long p, int len, int border) {
   if (p >= 0 && p < len) return (int)p;
+  // Coordinates just outside the image (the common case): no division.
+  if (p >= -(long long)len && p < 2LL * len && len > 1) {
+    const int q = (int)p;
+    switch (border) {
+      case kReplicate: return q < 0 ? 0 : len - 1;
+      case kReflect: return q < 0 ? -q - 1 : 2 * len - 1 - q;
+      case kReflect101:
+        if (q < 0 && q > -len) return -q;
+        if (q >= len && q < 2 * len - 1) return 2 * len - 2 - q;
+        break;
+      case kWrap: return q < 0 ? q + len : q - len;
+      default: break;
+    }
+  }
   switch (border) {
     case kConstant:
       return -1;
