@@ -1,0 +1,82 @@
+// Host-side tables shared by the per-call C ABI and the batch engine.
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <vector>
+
+#include "vb.h"
+
+namespace vb {
+
+// sat.cast(i16, f32) on the host.
+int sat_i16(float x) {
+  if (x != x) return 0;
+  const double r = std::nearbyint((double)x);
+  if (r <= -32768.0) return -32768;
+  if (r >= 32767.0) return 32767;
+  return (int)r;
+}
+
+// linearTapU8 (src/imgproc/resize.zig:181-214): OpenCV's 8-bit bilinear taps, the
+// source coordinate in f32 and each weight rounded to 11 bits on its own.
+LinTap lin_tap_u8(long long d, uint32_t ssize, uint32_t dsize, bool area, bool pin) {
+  const double inv = (double)dsize / (double)ssize;
+  const double scale = 1.0 / inv;
+  const double df = (double)d;
+  long long sx;
+  float fx;
+  if (area) {
+    sx = (long long)std::floor(df * scale);
+    fx = (float)((df + 1) - (double)(sx + 1) * inv);
+    fx = fx <= 0 ? 0.0f : fx - std::floor(fx);
+  } else {
+    fx = (float)((df + 0.5) * scale - 0.5);
+    const float fl = std::floor(fx);
+    sx = (long long)fl;
+    fx -= fl;
+  }
+  const long long last = (long long)ssize - 1;
+  if (pin && sx < 0) {
+    sx = 0;
+    fx = 0;
+  }
+  if (pin && sx >= last) {
+    sx = last;
+    fx = 0;
+  }
+  LinTap t;
+  t.w0 = sat_i16((1.0f - fx) * 2048.0f);
+  t.w1 = sat_i16(fx * 2048.0f);
+  t.o0 = (int)std::min(std::max(sx, 0LL), last);
+  t.o1 = (int)std::min(std::max(sx + 1, 0LL), last);
+  return t;
+}
+
+// getStructuringElement (src/imgproc/morph.zig:32-59).
+std::vector<uint8_t> structuring_element(int shape, int w, int h) {
+  std::vector<uint8_t> m((size_t)w * h, 0);
+  const int ax = w / 2, ay = h / 2;
+  const long long r = ay, c = ax;
+  const double inv_r2 = r > 0 ? 1.0 / (double)(r * r) : 0;
+  for (int i = 0; i < h; i++) {
+    int j1 = 0, j2 = 0;
+    if (shape == 0 || (shape == 1 && i == ay)) {
+      j2 = w;
+    } else if (shape == 1) {
+      j1 = ax;
+      j2 = j1 + 1;
+    } else {
+      const long long dy = (long long)i - r;
+      if (std::llabs(dy) <= r) {
+        const double dxf = (double)c * std::sqrt((double)(unsigned long long)(r * r - dy * dy) * inv_r2);
+        const long long dx = (long long)std::round(dxf);
+        j1 = (int)std::max(c - dx, 0LL);
+        j2 = (int)std::min(c + dx + 1, (long long)w);
+      }
+    }
+    for (int j = j1; j < j2; j++) m[(size_t)i * w + j] = 1;
+  }
+  return m;
+}
+
+}  // namespace vb

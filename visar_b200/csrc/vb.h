@@ -106,5 +106,11 @@ int gaussian_ksize(double sigma, bool depth_is_u8);
 void gaussian_kernel_fixed(int64_t *out, int n, double sigma, int bits);
 // getDerivKernels (src/imgproc/filter.zig:817-854). Returns false for an invalid kernel.
 bool deriv_kernel(int *out, int n, int order, int ksize);
+// sat.cast(i16, f32).
+int sat_i16(float x);
+// linearTapU8 (src/imgproc/resize.zig:181-214) for destination index d.
+LinTap lin_tap_u8(long long d, uint32_t ssize, uint32_t dsize, bool area, bool pin);
+// getStructuringElement (src/imgproc/morph.zig:32-59): h x w mask, row-major.
+std::vector<uint8_t> structuring_element(int shape, int w, int h);
 
 }  // namespace vb
