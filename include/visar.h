@@ -97,6 +97,18 @@ int visar_cuda_set_async(int async);
 /* Number of CUDA kernels the library launched since load (all threads). */
 uint64_t visar_cuda_launch_count(void);
 
+/* No counterpart in VISAR. visar_resize(src, dst, INTER_LINEAR) for uint8
+   images of 1-4 channels that both live in device memory, allocating no device
+   memory: the tap tables go to one 512 KiB buffer reserved statically per
+   device. Destination width and height are limited to 16384 (InvalidSize
+   beyond); host-resident or overlapping images are refused (InvalidArgument).
+   The buffer is shared by every call on a device, so two calls in flight at
+   once on one device race; issue them on one stream or one at a time. The
+   first call on a device resolves the buffer's address and should come before
+   any stream capture on that device. Same stream and async rules as the other
+   calls. */
+int visar_resize_linear_u8_noalloc(const visar_image *src, const visar_image *dst);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,131 @@
+"""visar_resize_linear_u8_noalloc against visar_resize(INTER_LINEAR).
+
+The allocation-free variant keeps its tap tables in one static device buffer;
+these tests hold its output equal to the per-call entry point's on calls made
+back to back (the second call rewrites the tables the first one used), check
+that repeated calls leave the device's free memory unchanged, and check the
+refusals (oversized destination, host or overlapping images, other depths).
+The file sorts last so that it also runs after every other test in the same
+process; it passes alone as well.
+"""
+import numpy as np
+import pytest
+
+import visar_b200 as vb
+from visar_b200 import synth
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+# (src h, w, channels, dst w, h): generic down/up scales, exact halving, same size.
+CASES = [
+    (480, 640, 3, 500, 333),
+    (37, 61, 1, 150, 90),
+    (1080, 1920, 4, 1280, 720),
+    (200, 300, 3, 100, 100),
+    (64, 64, 1, 32, 32),
+    (99, 77, 3, 77, 99),
+    (20, 30, 1, 30, 20),
+]
+
+
+def _src(h, w, c, seed):
+    img = synth.base_image(h, w, c, nrect=3, seed=seed)
+    return torch.from_numpy(img).cuda()
+
+
+def _dst(src, w, h):
+    c = src.shape[2] if src.ndim == 3 else 1
+    return torch.empty((h, w) if c == 1 else (h, w, c), dtype=torch.uint8, device=src.device)
+
+
+def test_matches_resize_on_consecutive_calls():
+    for i in range(len(CASES)):
+        a = CASES[i]
+        b = CASES[(i + 1) % len(CASES)]
+        sa, sb = _src(*a[:3], seed=100 + i), _src(*b[:3], seed=200 + i)
+        da, db = _dst(sa, a[3], a[4]), _dst(sb, b[3], b[4])
+        vb.resize_linear_u8_noalloc(sa, da)
+        vb.resize_linear_u8_noalloc(sb, db)
+        ra = vb.resize(sa, (a[3], a[4]), vb.INTER_LINEAR)
+        rb = vb.resize(sb, (b[3], b[4]), vb.INTER_LINEAR)
+        torch.cuda.synchronize()
+        assert torch.equal(da, ra), f"first call of pair {i}: {a}"
+        assert torch.equal(db, rb), f"second call of pair {i}: {b}"
+
+
+def test_consecutive_async_calls_on_one_stream():
+    s = torch.cuda.Stream()
+    srcs = [_src(*c[:3], seed=300 + k) for k, c in enumerate(CASES)]
+    dsts = [_dst(x, c[3], c[4]) for x, c in zip(srcs, CASES)]
+    torch.cuda.synchronize()
+    vb.set_stream(s.cuda_stream)
+    vb.set_async(1)
+    try:
+        for x, d in zip(srcs, dsts):
+            vb.resize_linear_u8_noalloc(x, d)
+    finally:
+        vb.set_async(0)
+        vb.set_stream(0)
+    s.synchronize()
+    for x, d, c in zip(srcs, dsts, CASES):
+        assert torch.equal(d, vb.resize(x, (c[3], c[4]), vb.INTER_LINEAR)), c
+
+
+def test_strided_rows():
+    base = _src(300, 500, 3, seed=7)
+    src = base[10:250, 20:420]  # rows keep the parent's stride
+    big = torch.zeros((200, 400, 3), dtype=torch.uint8, device="cuda")
+    dst = big[:, :333]
+    vb.resize_linear_u8_noalloc(src, dst)
+    ref = vb.resize(src.contiguous(), (333, 200), vb.INTER_LINEAR)
+    torch.cuda.synchronize()
+    assert torch.equal(dst, ref)
+    assert int(big[:, 333:].sum()) == 0
+
+
+def test_free_memory_unchanged():
+    srcs = [_src(*c[:3], seed=400 + k) for k, c in enumerate(CASES)]
+    dsts = [_dst(x, c[3], c[4]) for x, c in zip(srcs, CASES)]
+    # The first calls resolve the static buffer and load each kernel they use
+    # (module and function loading may reserve device memory once).
+    for x, d in zip(srcs, dsts):
+        vb.resize_linear_u8_noalloc(x, d)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(3):
+        for x, d in zip(srcs, dsts):
+            vb.resize_linear_u8_noalloc(x, d)
+    # A destination the per-call path has never been asked for.
+    odd = _dst(srcs[2], 16384, 3)
+    free1, _ = torch.cuda.mem_get_info()  # after torch's own allocation
+    vb.resize_linear_u8_noalloc(srcs[2], odd)
+    torch.cuda.synchronize()
+    free2, _ = torch.cuda.mem_get_info()
+    assert free1 <= free0
+    assert free2 == free1
+
+
+def test_refusals():
+    src = _src(40, 50, 3, seed=11)
+    with pytest.raises(vb.VisarError) as e:
+        vb.resize_linear_u8_noalloc(src, _dst(src, 16385, 2))
+    assert e.value.status == -1 and "InvalidSize" in e.value.name
+    with pytest.raises(vb.VisarError) as e:
+        vb.resize_linear_u8_noalloc(src, _dst(src, 2, 16385))
+    assert e.value.status == -1 and "InvalidSize" in e.value.name
+    host = src.cpu().numpy()
+    with pytest.raises(vb.VisarError) as e:
+        vb.resize_linear_u8_noalloc(host, np.empty((20, 25, 3), np.uint8))
+    assert e.value.status == -1
+    with pytest.raises(vb.VisarError) as e:
+        vb.resize_linear_u8_noalloc(src, src[:20, :25])
+    assert e.value.status == -1
+    f = torch.zeros((40, 50), dtype=torch.float32, device="cuda")
+    with pytest.raises(vb.VisarError) as e:
+        vb.resize_linear_u8_noalloc(f, torch.zeros((20, 25), dtype=torch.float32, device="cuda"))
+    assert e.value.status == -3
+    with pytest.raises(vb.VisarError) as e:
+        vb.resize_linear_u8_noalloc(src, _dst(_src(40, 50, 1, seed=1), 25, 20))
+    assert e.value.status == -2

@@ -171,6 +171,14 @@ def resize(a, size, interpolation=1, dst=None):
     return dst
 
 
+def resize_linear_u8_noalloc(a, dst):
+    """INTER_LINEAR resize of a uint8 CUDA tensor into `dst` (a CUDA tensor
+    the caller owns) through visar_resize_linear_u8_noalloc: no device memory
+    is allocated by the call; destination sides up to 16384."""
+    _check(lib.visar_resize_linear_u8_noalloc(ctypes.byref(desc(a)), ctypes.byref(desc(dst))))
+    return dst
+
+
 def gaussian_blur(a, ksize, sigma_x, sigma_y=0, border=4, dst=None):
     dst = _out(a, tuple(a.shape)) if dst is None else dst
     _check(lib.visar_gaussian_blur(ctypes.byref(desc(a)), ctypes.byref(desc(dst)), ksize[0], ksize[1],

@@ -1012,4 +1012,38 @@ int visar_warp_perspective(const visar_image *src, const visar_image *dst, const
   });
 }
 
+// visar_resize(src, dst, INTER_LINEAR) for u8 device images without any
+// device allocation: the tap tables go to a static device buffer
+// (noalloc.cu). Host images would need staging buffers and overlapping images
+// a private source copy, so both are refused rather than allocated.
+int visar_resize_linear_u8_noalloc(const visar_image *src, const visar_image *dst) {
+  return guarded([&] {
+    if (!src || !dst) invalid_arg();
+    if (src->depth != VISAR_8U || dst->depth != VISAR_8U) unsupported();
+    std::lock_guard<std::mutex> lk(g_mu);
+    View s = typed(src, k8U);
+    View d = typed(dst, k8U);
+    if (s.c->channels != d.c->channels) size_mismatch();
+    if (s.c->channels > 4) unsupported_channels();
+    if (s.host || d.host) fail(VISAR_INVALID_ARGUMENT, "InvalidArgument: noalloc resize needs device-resident images");
+    if (d.c->width > (uint32_t)kNoAllocMaxSide || d.c->height > (uint32_t)kNoAllocMaxSide)
+      fail(VISAR_INVALID_ARGUMENT, "InvalidSize: noalloc resize destination is limited to 16384 x 16384");
+    if (overlaps(s, d)) fail(VISAR_INVALID_ARGUMENT, "InvalidArgument: noalloc resize needs src and dst apart");
+    const int dev = t_hint_dev;
+    ck(cudaSetDevice(dev));
+    LinTap *taps = nullptr;
+    ck(static_taps_on_device(dev, &taps));
+    // The thread's stream, else the library's stream if it exists (no stream
+    // is created here), else the legacy default stream; ordered after the
+    // previous call's stream as begin_call orders calls.
+    DevCtx &c = g_ctx[dev];
+    const cudaStream_t st = t_stream ? t_stream : c.init ? c.own : cudaStreamLegacy;
+    if (c.last && c.last != st) ck(cudaStreamSynchronize(c.last));
+    c.last = st;
+    ck(launch_resize_linear_u8_static(s.dev, d.dev, taps, st));
+    ck(cudaGetLastError());
+    if (!t_async) ck(cudaStreamSynchronize(st));
+  });
+}
+
 }  // extern "C"

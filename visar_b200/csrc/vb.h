@@ -113,4 +113,10 @@ LinTap lin_tap_u8(long long d, uint32_t ssize, uint32_t dsize, bool area, bool p
 // getStructuringElement (src/imgproc/morph.zig:32-59): h x w mask, row-major.
 std::vector<uint8_t> structuring_element(int shape, int w, int h);
 
+// ------------------------------------- resize with a static tap buffer
+// Largest destination width or height of the allocation-free linear resize.
+constexpr int kNoAllocMaxSide = 16384;
+cudaError_t static_taps_on_device(int dev, LinTap **out);
+cudaError_t launch_resize_linear_u8_static(const DImg &s, const DImg &d, LinTap *taps, cudaStream_t st);
+
 }  // namespace vb
