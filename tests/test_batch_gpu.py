@@ -1,0 +1,187 @@
+"""The batched form (include/visar_batch.h) against the per-call drop-in.
+
+Every stage output of every image in a plan must equal, bit for bit, what
+the per-call entry points give for that image alone (which the parity suite
+holds equal to the oracle). Covers the mixed-size batch pipeline, a video
+frame pipeline replayed through a CUDA graph with new frames, every depth and
+channel count (including the images that take the per-call fallback), more
+images than the shared-memory prefix cache holds, and every tuning choice.
+"""
+import numpy as np
+import pytest
+
+import visar_b200 as vb
+from visar_b200 import batch as B
+from visar_b200 import synth
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+
+def dims_after_resize(h, w, fx, fy):
+    return max(1, round(h * fy)), max(1, round(w * fx))
+
+
+def plain_stage(x, spec):
+    """One stage through the per-call entry points (the reference of the batch)."""
+    kind, a = spec
+    c = 1 if x.ndim == 2 else x.shape[2]
+    if kind == "gray":
+        return x if c == 1 else vb.cvt_color(x, 6 if c == 3 else 10)
+    if kind == "gauss":
+        return vb.gaussian_blur(x, a["k"], a.get("sx", 0.0), a.get("sy", 0.0), a.get("border", 4))
+    if kind == "morph":
+        return vb.morphology(x, a["op"], a["shape"], a["k"], a.get("it", 1))
+    if kind == "resize":
+        h, w = dims_after_resize(x.shape[0], x.shape[1], a["fx"], a["fy"])
+        if (h, w) == tuple(x.shape[:2]):
+            return x
+        return vb.resize(x, (w, h), a.get("interp", 1))
+    if kind == "thresh":
+        return vb.threshold(x, a["t"], a["m"], a["type"])[1]
+    if kind == "affine":
+        return vb.warp_affine(x, a["m"][a["i"]], (x.shape[1], x.shape[0]), a.get("interp", 1), a.get("border", 0),
+                              a.get("value", 0.0))
+    if kind == "persp":
+        return vb.warp_perspective(x, a["m"][a["i"]], (x.shape[1], x.shape[0]), a.get("interp", 1),
+                                   a.get("border", 0), a.get("value", 0.0))
+    raise ValueError(kind)
+
+
+def batch_stage(spec):
+    kind, a = spec
+    if kind == "gray":
+        return B.gray()
+    if kind == "gauss":
+        return B.gaussian(a["k"], a.get("sx", 0.0), a.get("sy", 0.0), a.get("border", 4))
+    if kind == "morph":
+        return B.morphology(a["op"], a["shape"], a["k"], a.get("it", 1))
+    if kind == "resize":
+        return B.resize(a["fx"], a["fy"], a.get("interp", 1))
+    if kind == "thresh":
+        return B.threshold(a["t"], a["m"], a["type"])
+    if kind == "affine":
+        return B.warp_affine(None, a.get("interp", 1), a.get("border", 0), a.get("value", 0.0),
+                             per_image=np.stack(a["m"]))
+    if kind == "persp":
+        return B.warp_perspective(None, a.get("interp", 1), a.get("border", 0), a.get("value", 0.0),
+                                  per_image=np.stack(a["m"]))
+    raise ValueError(kind)
+
+
+def check_plan(images, specs, graph=False, plan=None):
+    plan = plan or B.Batch(images, [batch_stage(s) for s in specs])
+    (plan.run_graph if graph else plan.run)()
+    torch.cuda.synchronize()
+    for i, x in enumerate(images):
+        cur = x
+        for k, s in enumerate(specs):
+            if s[0] in ("affine", "persp"):
+                s = (s[0], dict(s[1], i=i))
+            cur = plain_stage(cur, s)
+            got = plan.stage_output(k, i)
+            assert tuple(got.shape) == tuple(cur.shape), (i, k, s[0])
+            if not torch.equal(got, cur):
+                bad = int((got != cur).sum())
+                raise AssertionError(f"image {i} {tuple(x.shape)} {x.dtype} stage {k} {s[0]}: {bad} samples differ")
+    return plan
+
+
+def mixed_u8(n, seed, wmax=1200, hmax=700, channels=(1, 3)):
+    shapes = synth.mixed_shapes(n, seed=seed, wmax=wmax, hmax=hmax, channels=channels)
+    return [synth.base_image_torch(h, w, c, nrect=8, seed=seed * 1000 + k) for k, (h, w, c) in enumerate(shapes)]
+
+
+C2 = [("gray", {}), ("gauss", {"k": (5, 5)}), ("morph", {"op": 2, "shape": 2, "k": (5, 5)}),
+      ("resize", {"fx": 0.5, "fy": 0.5})]
+
+
+def test_mixed_size_pipeline_matches_plain():
+    imgs = mixed_u8(24, seed=3)
+    # Degenerate and narrow shapes next to the large ones.
+    imgs += [synth.base_image_torch(h, w, c, nrect=1, seed=50 + k)
+             for k, (h, w, c) in enumerate([(1, 1, 1), (2, 3, 3), (64, 5, 1), (7, 300, 3), (3, 2, 1), (33, 17, 3)])]
+    plan = check_plan(imgs, C2)
+    info = plan.info()
+    assert info["images"] == len(imgs) and info["stages"] == 4
+    # One launch per shape class and pass: gray (3-ch), Gaussian (1-ch), erode + dilate, half + linear.
+    assert info["launches"] <= 8
+    check_plan(imgs, C2, graph=True, plan=plan)
+    check_plan(imgs, C2, graph=True, plan=plan)
+
+
+def test_video_frames_replayed_through_graph():
+    h, w = 360, 640
+    hom = synth.perspective_params(w, h, seed=7)
+    specs = [("gray", {}), ("gauss", {"k": (5, 5)}), ("thresh", {"t": 100, "m": 255, "type": 0}),
+             ("morph", {"op": 3, "shape": 0, "k": (7, 7)}), ("persp", {"m": [hom]})]
+    plan = B.Batch([(h, w, 3, np.uint8)], [batch_stage(s) for s in specs])
+    assert plan.info()["fallback_calls"] == 0
+    for f in range(3):
+        frame = synth.base_image_torch(h, w, 3, nrect=16, seed=100 + f)
+        plan.input(0).copy_(frame)
+        check_plan([frame], specs, graph=True, plan=plan)
+
+
+def test_depths_channels_and_fallbacks():
+    imgs, k = [], 0
+    for dt in (np.uint8, np.uint16, np.float32):
+        for c in (1, 3, 4):
+            for (h, w) in ((57, 91), (130, 64)):
+                x = synth.base_image(h, w, c, nrect=2, seed=200 + k, dtype=dt)
+                if dt == np.float32:
+                    x = synth.normal_f32(h, w, c, seed=200 + k)
+                imgs.append(torch.from_numpy(np.ascontiguousarray(x)).cuda())
+                k += 1
+    rng = np.random.default_rng(5)
+    mats = [synth.rotation_matrix_2d(x.shape[1] / 2, x.shape[0] / 2, rng.uniform(-30, 30), 1.0) for x in imgs]
+    specs = [("gauss", {"k": (5, 5)}), ("affine", {"m": mats}), ("morph", {"op": 2, "shape": 0, "k": (3, 3)}),
+             ("resize", {"fx": 0.5, "fy": 0.5}), ("gray", {})]
+    check_plan(imgs, specs)
+
+
+def test_thresholds_warps_and_borders():
+    imgs = mixed_u8(10, seed=11, wmax=400, hmax=300, channels=(1, 3, 4))
+    rng = np.random.default_rng(12)
+    homs = [synth.perspective_params(x.shape[1], x.shape[0], seed=300 + i) for i, x in enumerate(imgs)]
+    affs = [synth.affine_params(x.shape[1], x.shape[0], seed=400 + i) for i, x in enumerate(imgs)]
+    for t, typ in ((127, 0), (30, 1), (200, 2), (-5, 3), (300, 4)):
+        check_plan(imgs, [("thresh", {"t": t, "m": 255, "type": typ})])
+    for interp in (0, 1):
+        for border in (0, 1, 4):
+            check_plan(imgs, [("persp", {"m": homs, "interp": interp, "border": border, "value": 17}),
+                              ("affine", {"m": affs, "interp": interp, "border": border, "value": 250})])
+    for op, shape, k in ((0, 1, (3, 3)), (1, 2, (7, 7)), (3, 0, (9, 9)), (4, 0, (3, 3)), (2, 0, (11, 11))):
+        check_plan(imgs, [("morph", {"op": op, "shape": shape, "k": k, "it": 2})])
+    for k in ((3, 3), (7, 7), (9, 9)):
+        check_plan(imgs, [("gauss", {"k": k, "border": int(rng.integers(0, 5))})])
+    check_plan(imgs, [("resize", {"fx": 0.37, "fy": 0.61}), ("resize", {"fx": 1.7, "fy": 1.3}),
+                      ("resize", {"fx": 0.5, "fy": 0.5, "interp": 3})])
+
+
+def test_more_images_than_prefix_cache():
+    rng = np.random.default_rng(21)
+    imgs = []
+    for k in range(1100):
+        h, w, c = int(rng.integers(1, 30)), int(rng.integers(1, 40)), int(rng.choice([1, 3, 4]))
+        imgs.append(synth.base_image_torch(h, w, c, nrect=0, seed=k))
+    specs = [("gauss", {"k": (3, 3)}), ("morph", {"op": 1, "shape": 1, "k": (3, 3)}),
+             ("thresh", {"t": 90, "m": 200, "type": 0}), ("resize", {"fx": 0.5, "fy": 0.5})]
+    check_plan(imgs, specs)
+
+
+def test_tuning_choices_give_identical_results():
+    imgs = mixed_u8(8, seed=31, wmax=900, hmax=500)
+    try:
+        for rows in (8, 16, 32):
+            B.tune_set("gauss.u8.c1.k5.rows", rows)
+            B.tune_set("gauss.u8.c3.k5.rows", rows)
+            for er in (1, 3, 64):
+                for op in ("gray", "half", "linear", "lut"):
+                    for c in (0, 1, 3):
+                        B.tune_set(f"{op}.u8.c{c}.k0.rows", er)
+                B.tune_set("morph.u8.c1.k5.per_sm", 1 if er == 1 else 0)
+                check_plan(imgs, C2 + [("thresh", {"t": 128, "m": 255, "type": 0})])
+    finally:
+        B.tune_load(None)

@@ -1,0 +1,998 @@
+// Host side of the batched form (include/visar_batch.h): plan building,
+// shape classes, the device pool, launches, CUDA graph replay and the tuning
+// table. Device side: batch.cuh.
+#include <algorithm>
+#include <cerrno>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/visar_batch.h"
+#include "batch.cuh"
+
+namespace vb {
+namespace bt {
+namespace {
+
+// --------------------------------------------------------------- tuning
+
+std::mutex g_tune_mu;
+std::map<std::string, int> g_tune;
+
+int tune_get(const std::string &key, int fallback) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  const auto it = g_tune.find(key);
+  return it == g_tune.end() ? fallback : it->second;
+}
+
+// Reads the flat JSON object the autotuner writes: "key": integer pairs
+// (other values are skipped).
+bool parse_tune_json(const std::string &txt, std::map<std::string, int> &out) {
+  size_t i = 0;
+  const size_t n = txt.size();
+  while (i < n) {
+    const size_t q0 = txt.find('"', i);
+    if (q0 == std::string::npos) break;
+    const size_t q1 = txt.find('"', q0 + 1);
+    if (q1 == std::string::npos) return false;
+    const std::string key = txt.substr(q0 + 1, q1 - q0 - 1);
+    size_t j = q1 + 1;
+    while (j < n && (txt[j] == ' ' || txt[j] == '\t' || txt[j] == '\n' || txt[j] == '\r')) j++;
+    if (j < n && txt[j] == ':') {
+      j++;
+      while (j < n && (txt[j] == ' ' || txt[j] == '\t' || txt[j] == '\n' || txt[j] == '\r')) j++;
+      if (j < n && (txt[j] == '-' || (txt[j] >= '0' && txt[j] <= '9'))) {
+        char *end = nullptr;
+        const long v = std::strtol(txt.c_str() + j, &end, 10);
+        out[key] = (int)v;
+        j = (size_t)(end - txt.c_str());
+      } else if (j < n && txt[j] == '"') {
+        const size_t e = txt.find('"', j + 1);  // string value: skipped
+        if (e == std::string::npos) return false;
+        j = e + 1;
+      }
+    }
+    i = j;
+  }
+  return true;
+}
+
+// ----------------------------------------------------------------- plan
+
+struct Buf {
+  DImg v;
+  int depth;
+};
+
+enum OpKind { kOpGauss, kOpMorph, kOpGray, kOpHalf, kOpLinear, kOpLut, kOpWarpAff, kOpWarpPer };
+
+const char *op_name(int op) {
+  switch (op) {
+    case kOpGauss: return "gauss";
+    case kOpMorph: return "morph";
+    case kOpGray: return "gray";
+    case kOpHalf: return "half";
+    case kOpLinear: return "linear";
+    case kOpLut: return "lut";
+    case kOpWarpAff: return "warp_affine";
+    case kOpWarpPer: return "warp_perspective";
+  }
+  return "?";
+}
+
+// One persistent launch: one shape class of one stage pass.
+struct Launch {
+  int op = 0;
+  int depth = k8U;
+  int cn = 1;
+  int k = 0;        // kernel size (Gaussian) / element height (morphology)
+  bool is_max = false;
+  int rows = 8;     // tile rows (Gaussian band height, elementwise rows)
+  int per_sm = 0;   // CTAs per SM (0: as many as fit)
+  fast::FastArgs fa{};
+  fast::MFArgs ma{};
+  WarpArgs wa{};
+  const uint8_t *lut = nullptr;
+  std::vector<BImg> imgs;
+  size_t bytes = 0;  // algorithmic bytes
+  BImg *d_imgs = nullptr;
+  int *d_start = nullptr;
+  int total = 0;
+  int counter = 0;
+};
+
+// A per-image call through the per-call entry point.
+struct Fallback {
+  visar_stage st;
+  Buf s, d;
+  double m[9];
+};
+
+struct Step {
+  std::vector<Launch> launches;  // in order (morphology passes are ordered)
+  std::vector<Fallback> fallbacks;
+};
+
+// Device allocations of a plan: one block, sub-allocated.
+struct Pool {
+  uint8_t *base = nullptr;
+  size_t cap = 0, used = 0;
+  void *take(size_t bytes) {
+    const size_t off = (used + 255) & ~(size_t)255;
+    if (off + bytes > cap) return nullptr;
+    used = off + bytes;
+    return base + off;
+  }
+};
+
+}  // namespace
+
+struct Plan {
+  int dev = 0;
+  int num_sms = 148;
+  std::vector<Buf> inputs;
+  std::vector<std::vector<Buf>> outs;  // [stage][image]
+  std::vector<Step> steps;
+  Pool pool;
+  int *counters = nullptr;
+  int ncounters = 0;
+  size_t pixels_in = 0, bytes = 0, nlaunch = 0, nfallback = 0;
+  cudaStream_t own = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  ~Plan() {
+    if (graph) cudaGraphExecDestroy(graph);
+    if (pool.base) cudaFree(pool.base);
+    if (own) cudaStreamDestroy(own);
+  }
+};
+
+namespace {
+
+size_t pitch_of(long long rb) { return (size_t)((rb + 255) & ~255LL); }
+
+// Sizes the pool: first pass counts bytes, second pass takes them.
+struct Sizer {
+  size_t bytes = 0;
+  void add(size_t b) { bytes = ((bytes + 255) & ~(size_t)255) + b; }
+};
+
+struct Builder {
+  Plan &P;
+  bool sizing;
+  Sizer sz;
+  // Host copies of the per-launch device data, uploaded after the pool exists.
+  struct Upload {
+    void *dst;
+    std::vector<uint8_t> data;
+  };
+  std::vector<Upload> uploads;
+
+  void *take(size_t bytes) {
+    if (sizing) {
+      sz.add(bytes);
+      return nullptr;
+    }
+    return P.pool.take(bytes);
+  }
+  bool image(int w, int h, int cn, int depth, Buf &out) {
+    const size_t pitch = pitch_of((long long)w * cn * depth_size(depth));
+    void *p = take(pitch * (size_t)h);
+    if (!sizing && !p) return false;
+    out = Buf{DImg{static_cast<uint8_t *>(p), (long long)pitch, w, h, cn}, depth};
+    return true;
+  }
+  template <class T>
+  T *table(const std::vector<T> &v) {
+    const size_t bytes = sizeof(T) * std::max<size_t>(1, v.size());
+    void *p = take(bytes);
+    if (sizing || !p) return static_cast<T *>(p);
+    Upload u;
+    u.dst = p;
+    u.data.resize(bytes);
+    if (!v.empty()) std::memcpy(u.data.data(), v.data(), sizeof(T) * v.size());
+    uploads.push_back(std::move(u));
+    return static_cast<T *>(p);
+  }
+};
+
+std::string size_class(const std::vector<BImg> &imgs, int op) {
+  // Mean destination pixels of the class: S < 0.25 MP <= M < 2 MP <= L.
+  double px = 0;
+  for (const BImg &b : imgs) px += (double)b.d.w * b.d.h;
+  px /= std::max<size_t>(1, imgs.size());
+  (void)op;
+  return px < 250e3 ? "S" : px < 2e6 ? "M" : "L";
+}
+
+std::string launch_key(const Launch &L) {
+  char buf[96];
+  std::snprintf(buf, sizeof(buf), "%s.%s.c%d.k%d", op_name(L.op), L.depth == k32F ? "f32" : "u8", L.cn, L.k);
+  return buf;
+}
+
+Launch *class_of(std::vector<Launch> &ls, int op, int depth, int cn, int k, bool is_max) {
+  for (Launch &l : ls)
+    if (l.op == op && l.depth == depth && l.cn == cn && l.k == k && l.is_max == is_max) return &l;
+  ls.emplace_back();
+  Launch &l = ls.back();
+  l.op = op;
+  l.depth = depth;
+  l.cn = cn;
+  l.k = k;
+  l.is_max = is_max;
+  return &l;
+}
+
+int gauss_tiles_x(int w, int cn, int k) {
+  const int hw = ((k / 2) * cn + 3) / 4;
+  return (int)ceil_div(((long long)w * cn + 3) / 4, 128 - 2 * hw);
+}
+
+// Tiles per image of an operation, for the launch's tuned parameters.
+void set_tiles(const Launch &L, BImg &b) {
+  switch (L.op) {
+    case kOpGauss:
+      b.tiles_x = gauss_tiles_x(b.s.w, L.cn, L.k);
+      b.tiles_y = (int)ceil_div(b.s.h, L.rows);
+      break;
+    case kOpMorph:
+      b.tiles_x = (int)ceil_div(((long long)b.s.w * L.cn + 3) / 4, 126);
+      b.tiles_y = (int)ceil_div(b.s.h, 8);
+      break;
+    case kOpGray:
+      b.tiles_x = (int)ceil_div(b.s.w, 256 * 16);
+      b.tiles_y = (int)ceil_div(b.s.h, L.rows);
+      break;
+    case kOpHalf:
+      b.tiles_x = (int)ceil_div(b.d.w, 256 * 4);
+      b.tiles_y = (int)ceil_div(b.d.h, L.rows);
+      break;
+    case kOpLinear:
+      b.tiles_x = (int)ceil_div(b.d.w, 256);
+      b.tiles_y = (int)ceil_div(b.d.h, L.rows);
+      break;
+    case kOpLut:
+      b.tiles_x = (int)ceil_div((long long)b.s.w * b.s.cn, 256 * 16);
+      b.tiles_y = (int)ceil_div(b.s.h, L.rows);
+      break;
+    default:
+      b.tiles_x = (int)ceil_div(b.d.w, 32);
+      b.tiles_y = (int)ceil_div(b.d.h, 32);
+  }
+}
+
+// Applies the tuning table to a finished class, then tiles its images.
+void tune_and_tile(Launch &L) {
+  const std::string key = launch_key(L);
+  const std::string sc = size_class(L.imgs, L.op);
+  auto get = [&](const char *field, int def) {
+    return tune_get(key + "." + sc + "." + field, tune_get(key + "." + field, def));
+  };
+  switch (L.op) {
+    case kOpGauss: {
+      const int r = get("rows", 16);
+      L.rows = r == 8 || r == 16 || r == 32 ? r : 16;
+      break;
+    }
+    case kOpGray: case kOpHalf: case kOpLinear: case kOpLut: {
+      const int r = get("rows", 8);
+      L.rows = std::min(std::max(r, 1), 64);
+      break;
+    }
+    default: L.rows = 8;
+  }
+  L.per_sm = std::max(0, get("per_sm", 0));
+  for (BImg &b : L.imgs) set_tiles(L, b);
+}
+
+bool u8_aligned4(const DImg &v) { return ((uintptr_t)v.p % 4 == 0) && (v.stride % 4 == 0); }
+bool aligned16(const DImg &v) { return ((uintptr_t)v.p % 16 == 0) && (v.stride % 16 == 0); }
+
+BImg bimg(const DImg &s, const DImg &d) {
+  BImg b{};
+  b.s = s;
+  b.d = d;
+  return b;
+}
+
+void u8_bytes(Launch &L, const DImg &s, const DImg &d, int esize) {
+  L.bytes += ((size_t)s.w * s.h * s.cn + (size_t)d.w * d.h * d.cn) * (size_t)esize;
+}
+
+// ------------------------------------------------------------- stages
+
+// Builds one stage over `cur`, writing its outputs to `next`. Returns a
+// VISAR status.
+int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, std::vector<Buf> &next, Step &step) {
+  const size_t n = cur.size();
+  next.resize(n);
+  std::vector<Launch> ls;
+  auto fallback = [&](size_t i, const Buf &out, const double *m) {
+    Fallback f;
+    f.st = st;
+    f.s = cur[i];
+    f.d = out;
+    std::memset(f.m, 0, sizeof(f.m));
+    if (m) std::memcpy(f.m, m, sizeof(double) * (st.kind == VISAR_STAGE_WARP_AFFINE ? 6 : 9));
+    step.fallbacks.push_back(f);
+  };
+  switch (st.kind) {
+    case VISAR_STAGE_GRAY: {
+      for (size_t i = 0; i < n; i++) {
+        const Buf &im = cur[i];
+        if (im.v.cn == 1) {
+          next[i] = im;
+          continue;
+        }
+        if (im.v.cn != 3 && im.v.cn != 4) return VISAR_UNSUPPORTED;
+        if (!B.image(im.v.w, im.v.h, 1, im.depth, next[i])) return VISAR_OUT_OF_MEMORY;
+        if (im.depth != k8U) {
+          fallback(i, next[i], nullptr);
+          continue;
+        }
+        Launch *l = class_of(ls, kOpGray, k8U, im.v.cn, 0, false);
+        l->imgs.push_back(bimg(im.v, next[i].v));
+        u8_bytes(*l, im.v, next[i].v, 1);
+      }
+      break;
+    }
+    case VISAR_STAGE_GAUSSIAN: {
+      const int kw_in = st.i[0], kh_in = st.i[1], border = st.i[2];
+      const double sx = st.d[0], sy = st.d[1] > 0 ? st.d[1] : st.d[0];
+      if (border < 0 || border > 4) return VISAR_UNSUPPORTED;
+      if (kw_in < 0 || kh_in < 0) return VISAR_INVALID_ARGUMENT;
+      for (size_t i = 0; i < n; i++) {
+        const Buf &im = cur[i];
+        if (!B.image(im.v.w, im.v.h, im.v.cn, im.depth, next[i])) return VISAR_OUT_OF_MEMORY;
+        const bool u8 = im.depth == k8U;
+        const int kw = kw_in > 0 ? kw_in : gaussian_ksize(sx, u8);
+        const int kh = kh_in > 0 ? kh_in : gaussian_ksize(sy, u8);
+        if (kw <= 0 || kh <= 0 || kw % 2 == 0 || kh % 2 == 0 || kw > 127 || kh > 127) return VISAR_INVALID_ARGUMENT;
+        bool ok = (im.depth == k8U || im.depth == k32F) && kw == kh && sx == sy && (kw == 3 || kw == 5 || kw == 7) &&
+                  (im.v.cn == 1 || im.v.cn == 3 || im.v.cn == 4) && im.v.w > 1 && im.v.h > 1;
+        ok = ok && (u8 ? u8_aligned4(im.v) : aligned16(im.v));
+        fast::FastArgs a{};
+        if (ok) {
+          a.border = border;
+          a.symx = a.symy = 1;
+          if (u8) {
+            std::vector<int64_t> t(kw);
+            gaussian_kernel_fixed(t.data(), kw, sx, 8);
+            long long sum = 0;
+            for (int j = 0; j < kw; j++) {
+              ok = ok && t[j] >= 0 && t[j] == t[kw - 1 - j];
+              sum += t[j];
+              a.kx[j] = a.ky[j] = (float)t[j];
+            }
+            ok = ok && sum <= 256;
+            a.shift = 16;
+          } else {
+            std::vector<double> t(kw);
+            gaussian_kernel(t.data(), kw, sx);
+            for (int j = 0; j < kw; j++) {
+              const float f = (float)t[j];
+              ok = ok && f >= 0.0f && f == (float)t[kw - 1 - j];
+              a.kx[j] = a.ky[j] = f;
+            }
+          }
+        }
+        if (!ok) {
+          fallback(i, next[i], nullptr);
+          continue;
+        }
+        Launch *l = class_of(ls, kOpGauss, im.depth, im.v.cn, kw, false);
+        l->fa = a;
+        l->imgs.push_back(bimg(im.v, next[i].v));
+        u8_bytes(*l, im.v, next[i].v, depth_size(im.depth));
+      }
+      break;
+    }
+    case VISAR_STAGE_MORPHOLOGY: {
+      const int op = st.i[0], shape = st.i[1], kw = st.i[2], kh = st.i[3], it = st.i[4];
+      if (op < 0 || op > 6 || shape < 0 || shape > 2) return VISAR_UNSUPPORTED;
+      if (kw <= 0 || kh <= 0 || kw > 255 || kh > 255 || it < 0) return VISAR_INVALID_ARGUMENT;
+      const std::vector<uint8_t> mask = structuring_element(shape, kw, kh);
+      // The passes of ops 0-3 (morph.zig:71-96, 560-593): erode/dilate `it` times each.
+      std::vector<bool> passes;
+      auto add = [&](bool mx) {
+        for (int j = 0; j < it; j++) passes.push_back(mx);
+      };
+      if (op == 0) add(false);
+      else if (op == 1) add(true);
+      else if (op == 2) { add(false); add(true); }
+      else if (op == 3) { add(true); add(false); }
+      const bool kernel_ok = op <= 3 && !passes.empty();
+      std::vector<std::vector<Buf>> tmp(n);
+      std::vector<bool> fast_img(n, false);
+      for (size_t i = 0; i < n; i++) {
+        const Buf &im = cur[i];
+        if (!B.image(im.v.w, im.v.h, im.v.cn, im.depth, next[i])) return VISAR_OUT_OF_MEMORY;
+        fast::MFArgs ma;
+        fast_img[i] = kernel_ok && im.depth == k8U && fast::morph_fast_args(mask, kw, kh, im.v.cn, im.v.w, ma) &&
+                      u8_aligned4(im.v);
+        if (!fast_img[i]) {
+          fallback(i, next[i], nullptr);
+          continue;
+        }
+        const size_t ntmp = std::min<size_t>(passes.size() - 1, 2);
+        tmp[i].resize(ntmp);
+        for (size_t k = 0; k < ntmp; k++)
+          if (!B.image(im.v.w, im.v.h, im.v.cn, im.depth, tmp[i][k])) return VISAR_OUT_OF_MEMORY;
+      }
+      const size_t np = passes.size();
+      for (size_t p = 0; p < np && kernel_ok; p++) {
+        std::vector<Launch> pl;
+        for (size_t i = 0; i < n; i++) {
+          if (!fast_img[i]) continue;
+          const Buf &im = cur[i];
+          const DImg src = p == 0 ? im.v : tmp[i][(p - 1) % 2].v;
+          const DImg dst = p + 1 == np ? next[i].v : tmp[i][p % 2].v;
+          Launch *l = class_of(pl, kOpMorph, k8U, im.v.cn, kh, passes[p]);
+          fast::morph_fast_args(mask, kw, kh, im.v.cn, im.v.w, l->ma);
+          l->imgs.push_back(bimg(src, dst));
+          u8_bytes(*l, src, dst, 1);
+        }
+        for (Launch &l : pl) {
+          tune_and_tile(l);
+          step.launches.push_back(std::move(l));
+        }
+      }
+      return VISAR_OK;
+    }
+    case VISAR_STAGE_RESIZE: {
+      const int interp = st.i[0];
+      const double fx = st.d[0], fy = st.d[1];
+      if (interp < 0 || interp > 4) return VISAR_UNSUPPORTED;
+      if (!(fx > 0) || !(fy > 0) || !std::isfinite(fx) || !std::isfinite(fy)) return VISAR_INVALID_ARGUMENT;
+      for (size_t i = 0; i < n; i++) {
+        const Buf &im = cur[i];
+        const double wd = std::nearbyint((double)im.v.w * fx), hd = std::nearbyint((double)im.v.h * fy);
+        if (wd > 1e9 || hd > 1e9) return VISAR_INVALID_ARGUMENT;
+        const int dw = std::max(1, (int)wd), dh = std::max(1, (int)hd);
+        if (dw == im.v.w && dh == im.v.h && interp != 4) {
+          next[i] = im;  // VISAR copies; the pixels are the input's
+          continue;
+        }
+        if (interp == 4) return VISAR_UNSUPPORTED;
+        if (!B.image(dw, dh, im.v.cn, im.depth, next[i])) return VISAR_OUT_OF_MEMORY;
+        const bool u8lin = im.depth == k8U && im.v.cn <= 4 && interp == 1;
+        if (!u8lin) {
+          fallback(i, next[i], nullptr);
+          continue;
+        }
+        if (im.v.w == 2 * dw && im.v.h == 2 * dh) {
+          Launch *l = class_of(ls, kOpHalf, k8U, im.v.cn, 0, false);
+          l->imgs.push_back(bimg(im.v, next[i].v));
+          u8_bytes(*l, im.v, next[i].v, 1);
+        } else {
+          std::vector<LinTap> xt(dw), yt(dh);
+          for (int x = 0; x < dw; x++) xt[x] = lin_tap_u8(x, im.v.w, dw, false, true);
+          for (int y = 0; y < dh; y++) yt[y] = lin_tap_u8(y, im.v.h, dh, false, false);
+          BImg b = bimg(im.v, next[i].v);
+          b.t0 = B.table(xt);
+          b.t1 = B.table(yt);
+          if (!B.sizing && (!b.t0 || !b.t1)) return VISAR_OUT_OF_MEMORY;
+          Launch *l = class_of(ls, kOpLinear, k8U, im.v.cn, 0, false);
+          l->imgs.push_back(b);
+          u8_bytes(*l, im.v, next[i].v, 1);
+        }
+      }
+      break;
+    }
+    case VISAR_STAGE_THRESHOLD: {
+      const int type = st.i[0];
+      const int kind = type & 7;
+      if (kind > 4) return VISAR_UNSUPPORTED;
+      const bool autoth = (type & 24) != 0;
+      const double fl = std::floor(st.d[0]);
+      const int ti = fl != fl ? 0 : fl < -1e9 ? -1000000000 : fl > 1e9 ? 1000000000 : (int)fl;
+      const double r = std::nearbyint(st.d[1]);
+      const uint8_t m = st.d[1] != st.d[1] ? 0 : r <= 0 ? 0 : r >= 255 ? 255 : (uint8_t)(int)r;
+      // threshold.zig:39-60: the u8 table of every type.
+      std::vector<uint8_t> lut(256);
+      const uint8_t tsat = (uint8_t)std::min(std::max(ti, 0), 255);
+      for (int v = 0; v < 256; v++) {
+        const bool gt = v > ti;
+        switch (kind) {
+          case 0: lut[v] = gt ? m : 0; break;
+          case 1: lut[v] = gt ? 0 : m; break;
+          case 2: lut[v] = gt ? tsat : (uint8_t)v; break;
+          case 3: lut[v] = gt ? (uint8_t)v : 0; break;
+          default: lut[v] = gt ? 0 : (uint8_t)v; break;
+        }
+      }
+      const uint8_t *dlut = nullptr;
+      for (size_t i = 0; i < n; i++) {
+        const Buf &im = cur[i];
+        if (!B.image(im.v.w, im.v.h, im.v.cn, im.depth, next[i])) return VISAR_OUT_OF_MEMORY;
+        if (im.depth != k8U || autoth) {
+          fallback(i, next[i], nullptr);
+          continue;
+        }
+        if (!dlut) {
+          dlut = B.table(lut);
+          if (!B.sizing && !dlut) return VISAR_OUT_OF_MEMORY;
+        }
+        Launch *l = class_of(ls, kOpLut, k8U, 0, 0, false);
+        l->lut = dlut;
+        l->imgs.push_back(bimg(im.v, next[i].v));
+        u8_bytes(*l, im.v, next[i].v, 1);
+      }
+      break;
+    }
+    case VISAR_STAGE_WARP_AFFINE:
+    case VISAR_STAGE_WARP_PERSPECTIVE: {
+      const bool persp = st.kind == VISAR_STAGE_WARP_PERSPECTIVE;
+      const int interp = st.i[0] == 0 ? 0 : 1, border = st.i[1];
+      if (border < 0 || border > 4) return VISAR_UNSUPPORTED;
+      const double value = persp ? st.d[9] : st.d[6];
+      const int nm = persp ? 9 : 6;
+      for (size_t i = 0; i < n; i++) {
+        const Buf &im = cur[i];
+        const double *m = st.per_image ? st.per_image + i * nm : st.d;
+        BImg b = bimg(im.v, DImg{});
+        if (persp) {
+          if (!perspective_inverse(m, b.md)) return VISAR_UNSUPPORTED;
+        } else {
+          if (!affine_inverse_f32(m, b.mf)) return VISAR_UNSUPPORTED;
+        }
+        if (!B.image(im.v.w, im.v.h, im.v.cn, im.depth, next[i])) return VISAR_OUT_OF_MEMORY;
+        b.d = next[i].v;
+        const bool ok = (im.depth == k8U || im.depth == k32F) && (im.v.cn == 1 || im.v.cn == 3 || im.v.cn == 4) &&
+                        (im.depth != k8U || im.v.cn != 4 || u8_aligned4(im.v)) &&
+                        (im.depth != k32F || ((uintptr_t)im.v.p % 4 == 0 && im.v.stride % 4 == 0));
+        if (!ok) {
+          fallback(i, next[i], m);
+          continue;
+        }
+        b.cv = im.depth == k8U ? wp::sat_value_host<uint8_t>(value) : wp::sat_value_host<float>(value);
+        b.wide = ((uintptr_t)im.v.p % 8 == 0) && (im.v.stride % 8 == 0);
+        Launch *l = class_of(ls, persp ? kOpWarpPer : kOpWarpAff, im.depth, im.v.cn, 0, false);
+        l->wa = WarpArgs{interp, border};
+        l->imgs.push_back(b);
+        u8_bytes(*l, im.v, next[i].v, depth_size(im.depth));
+      }
+      break;
+    }
+    default:
+      return VISAR_UNSUPPORTED;
+  }
+  for (Launch &l : ls) {
+    tune_and_tile(l);
+    step.launches.push_back(std::move(l));
+  }
+  return VISAR_OK;
+}
+
+int build_all(Builder &B, const std::vector<visar_stage> &stages) {
+  Plan &P = B.P;
+  P.steps.clear();
+  P.outs.clear();
+  std::vector<Buf> cur = P.inputs;
+  for (const visar_stage &st : stages) {
+    Step step;
+    std::vector<Buf> next;
+    const int rc = build_stage(B, st, cur, next, step);
+    if (rc != VISAR_OK) return rc;
+    P.steps.push_back(std::move(step));
+    P.outs.push_back(next);
+    cur = next;
+  }
+  return VISAR_OK;
+}
+
+// ------------------------------------------------------------------ run
+
+std::mutex g_kattr_mu;
+std::map<const void *, int> g_occ;
+
+template <class Op>
+cudaError_t run_op(const Plan &P, const Launch &L, const typename Op::Args &a, cudaStream_t st) {
+  const TileQ q{L.d_imgs, L.d_start, (int)L.imgs.size(), L.total, P.counters + L.counter};
+  const size_t smem = Op::smem(a);
+  auto kern = k_batch<Op>;
+  int occ = 0;
+  {
+    std::lock_guard<std::mutex> lk(g_kattr_mu);
+    const auto it = g_occ.find((const void *)kern);
+    if (it == g_occ.end()) {
+      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, Op::kThreads, smem);
+      if (e != cudaSuccess) return e;
+      g_occ[(const void *)kern] = occ;
+    } else {
+      occ = it->second;
+    }
+  }
+  const int per_sm = L.per_sm > 0 ? std::min(L.per_sm, std::max(occ, 1)) : std::max(occ, 1);
+  const int grid = std::max(1, std::min(L.total, P.num_sms * per_sm));
+  kern<<<grid, Op::kThreads, smem, st>>>(q, a);
+  note_launch();
+  return cudaGetLastError();
+}
+
+template <class S, int K, int CN>
+cudaError_t run_gauss_rows(const Plan &P, const Launch &L, cudaStream_t st) {
+  switch (L.rows) {
+    case 8: return run_op<OpGauss<S, K, CN, 8>>(P, L, L.fa, st);
+    case 32: return run_op<OpGauss<S, K, CN, 32>>(P, L, L.fa, st);
+    default: return run_op<OpGauss<S, K, CN, 16>>(P, L, L.fa, st);
+  }
+}
+
+template <class S, int CN>
+cudaError_t run_gauss_k(const Plan &P, const Launch &L, cudaStream_t st) {
+  switch (L.k) {
+    case 3: return run_gauss_rows<S, 3, CN>(P, L, st);
+    case 5: return run_gauss_rows<S, 5, CN>(P, L, st);
+    case 7: return run_gauss_rows<S, 7, CN>(P, L, st);
+  }
+  return cudaErrorNotSupported;
+}
+
+template <class S>
+cudaError_t run_gauss(const Plan &P, const Launch &L, cudaStream_t st) {
+  switch (L.cn) {
+    case 1: return run_gauss_k<S, 1>(P, L, st);
+    case 3: return run_gauss_k<S, 3>(P, L, st);
+    case 4: return run_gauss_k<S, 4>(P, L, st);
+  }
+  return cudaErrorNotSupported;
+}
+
+template <int CN, bool MAX>
+cudaError_t run_morph_kh(const Plan &P, const Launch &L, cudaStream_t st) {
+  switch (L.k) {
+    case 1: return run_op<OpMorph<CN, 1, MAX>>(P, L, L.ma, st);
+    case 3: return run_op<OpMorph<CN, 3, MAX>>(P, L, L.ma, st);
+    case 5: return run_op<OpMorph<CN, 5, MAX>>(P, L, L.ma, st);
+    case 7: return run_op<OpMorph<CN, 7, MAX>>(P, L, L.ma, st);
+    case 9: return run_op<OpMorph<CN, 9, MAX>>(P, L, L.ma, st);
+  }
+  return cudaErrorNotSupported;
+}
+
+template <int CN>
+cudaError_t run_morph(const Plan &P, const Launch &L, cudaStream_t st) {
+  return L.is_max ? run_morph_kh<CN, true>(P, L, st) : run_morph_kh<CN, false>(P, L, st);
+}
+
+template <class T, bool PERSP>
+cudaError_t run_warp(const Plan &P, const Launch &L, cudaStream_t st) {
+  switch (L.cn) {
+    case 1: return run_op<OpWarp<T, 1, PERSP>>(P, L, L.wa, st);
+    case 3: return run_op<OpWarp<T, 3, PERSP>>(P, L, L.wa, st);
+    case 4: return run_op<OpWarp<T, 4, PERSP>>(P, L, L.wa, st);
+  }
+  return cudaErrorNotSupported;
+}
+
+cudaError_t run_launch(const Plan &P, const Launch &L, cudaStream_t st) {
+  if (L.total == 0) return cudaSuccess;
+  const RowArgs ra{L.rows};
+  switch (L.op) {
+    case kOpGauss: return L.depth == k8U ? run_gauss<uint8_t>(P, L, st) : run_gauss<float>(P, L, st);
+    case kOpMorph:
+      if (L.cn == 1) return run_morph<1>(P, L, st);
+      if (L.cn == 3) return run_morph<3>(P, L, st);
+      return run_morph<4>(P, L, st);
+    case kOpGray: return L.cn == 3 ? run_op<OpGray<3>>(P, L, ra, st) : run_op<OpGray<4>>(P, L, ra, st);
+    case kOpHalf:
+      switch (L.cn) {
+        case 1: return run_op<OpHalf<1>>(P, L, ra, st);
+        case 2: return run_op<OpHalf<2>>(P, L, ra, st);
+        case 3: return run_op<OpHalf<3>>(P, L, ra, st);
+        default: return run_op<OpHalf<4>>(P, L, ra, st);
+      }
+    case kOpLinear:
+      switch (L.cn) {
+        case 1: return run_op<OpLinear<1>>(P, L, ra, st);
+        case 2: return run_op<OpLinear<2>>(P, L, ra, st);
+        case 3: return run_op<OpLinear<3>>(P, L, ra, st);
+        default: return run_op<OpLinear<4>>(P, L, ra, st);
+      }
+    case kOpLut: return run_op<OpLut>(P, L, LutArgs{L.rows, L.lut}, st);
+    case kOpWarpAff: return L.depth == k8U ? run_warp<uint8_t, false>(P, L, st) : run_warp<float, false>(P, L, st);
+    case kOpWarpPer: return L.depth == k8U ? run_warp<uint8_t, true>(P, L, st) : run_warp<float, true>(P, L, st);
+  }
+  return cudaErrorNotSupported;
+}
+
+visar_image cimg(const Buf &b) {
+  visar_image c;
+  c.width = (uint32_t)b.v.w;
+  c.height = (uint32_t)b.v.h;
+  c.channels = (uint32_t)b.v.cn;
+  c.depth = (uint32_t)b.depth;
+  c.stride = (size_t)b.v.stride;
+  c.data = b.v.p;
+  return c;
+}
+
+int run_fallback(const Fallback &f) {
+  const visar_image s = cimg(f.s), d = cimg(f.d);
+  const visar_stage &st = f.st;
+  switch (st.kind) {
+    case VISAR_STAGE_GRAY: return visar_cvt_color(&s, &d, f.s.v.cn == 4 ? 10 : 6);
+    case VISAR_STAGE_GAUSSIAN: return visar_gaussian_blur(&s, &d, st.i[0], st.i[1], st.d[0], st.d[1], st.i[2]);
+    case VISAR_STAGE_MORPHOLOGY: return visar_morphology(&s, &d, st.i[0], st.i[1], st.i[2], st.i[3], st.i[4]);
+    case VISAR_STAGE_RESIZE: return visar_resize(&s, &d, st.i[0]);
+    case VISAR_STAGE_THRESHOLD: return visar_threshold(&s, &d, st.d[0], st.d[1], st.i[0], nullptr);
+    case VISAR_STAGE_WARP_AFFINE: return visar_warp_affine(&s, &d, f.m, st.i[0], st.i[1], st.d[6]);
+    case VISAR_STAGE_WARP_PERSPECTIVE: return visar_warp_perspective(&s, &d, f.m, st.i[0], st.i[1], st.d[9]);
+  }
+  return VISAR_UNSUPPORTED;
+}
+
+int cuda_status(cudaError_t e) {
+  if (e == cudaSuccess) return VISAR_OK;
+  static thread_local char buf[160];
+  std::snprintf(buf, sizeof(buf), "CudaError: %s", cudaGetErrorName(e));
+  if (e == cudaErrorMemoryAllocation) return report_error(VISAR_OUT_OF_MEMORY, "OutOfMemory");
+  return report_error(VISAR_INTERNAL, buf);
+}
+
+// Enqueues the whole plan on st. Fallback calls run on st in async mode.
+int enqueue(Plan &P, cudaStream_t st) {
+  if (P.ncounters > 0) {
+    const cudaError_t e = cudaMemsetAsync(P.counters, 0, sizeof(int) * (size_t)P.ncounters, st);
+    if (e != cudaSuccess) return cuda_status(e);
+  }
+  for (const Step &s : P.steps) {
+    for (const Launch &L : s.launches) {
+      const cudaError_t e = run_launch(P, L, st);
+      if (e != cudaSuccess) return cuda_status(e);
+    }
+    if (!s.fallbacks.empty()) {
+      const cudaStream_t old = thread_stream();
+      const int old_async = thread_async();
+      set_thread_stream(st, 1);
+      int rc = VISAR_OK;
+      for (const Fallback &f : s.fallbacks) {
+        rc = run_fallback(f);
+        if (rc != VISAR_OK) break;
+      }
+      set_thread_stream(old, old_async);
+      if (rc != VISAR_OK) return rc;
+    }
+  }
+  return VISAR_OK;
+}
+
+cudaStream_t run_stream(Plan &P) {
+  const cudaStream_t t = thread_stream();
+  return t ? t : P.own;
+}
+
+int finish(cudaStream_t st) {
+  if (thread_async()) return VISAR_OK;
+  return cuda_status(cudaStreamSynchronize(st));
+}
+
+}  // namespace
+}  // namespace bt
+}  // namespace vb
+
+using namespace vb;
+using namespace vb::bt;
+
+struct visar_batch {
+  Plan plan;
+};
+
+extern "C" {
+
+int visar_batch_create(const visar_image *inputs, size_t n, const visar_stage *stages, size_t nstages,
+                       visar_batch **out) {
+  if (!out || (n > 0 && !inputs) || (nstages > 0 && !stages) || n > (size_t)INT32_MAX)
+    return report_error(VISAR_INVALID_ARGUMENT, "InvalidArgument");
+  *out = nullptr;
+  std::unique_ptr<visar_batch> b(new (std::nothrow) visar_batch);
+  if (!b) return report_error(VISAR_OUT_OF_MEMORY, "OutOfMemory");
+  Plan &P = b->plan;
+  // Inputs: device images of one device, or plan-owned (data == NULL).
+  int dev = -1;
+  for (size_t i = 0; i < n; i++) {
+    const visar_image &c = inputs[i];
+    if (!(c.depth == 0 || c.depth == 2 || c.depth == 3 || c.depth == 5)) return report_error(VISAR_UNSUPPORTED, "Unsupported");
+    if (c.channels == 0 || c.channels > 4) return report_error(VISAR_UNSUPPORTED, "UnsupportedChannels");
+    if (c.width == 0 || c.height == 0 || c.width > (1u << 30) || c.height > (1u << 30))
+      return report_error(VISAR_INVALID_ARGUMENT, "InvalidSize");
+    if (!c.data) continue;
+    const int es = depth_size((int)c.depth);
+    if (c.stride % es != 0 || c.stride < (size_t)c.width * c.channels * es) return report_error(VISAR_INVALID_ARGUMENT, "InvalidSize");
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, c.data) != cudaSuccess || !(a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged)) {
+      cudaGetLastError();
+      return report_error(VISAR_INVALID_ARGUMENT, "InvalidArgument: batch inputs must be device memory");
+    }
+    if (dev >= 0 && a.device != dev) return report_error(VISAR_INVALID_ARGUMENT, "InvalidArgument: batch inputs on several devices");
+    dev = a.device;
+  }
+  if (dev < 0 && cudaGetDevice(&dev) != cudaSuccess) return cuda_status(cudaGetLastError());
+  cudaError_t e = cudaSetDevice(dev);
+  if (e != cudaSuccess) return cuda_status(e);
+  P.dev = dev;
+  cudaDeviceGetAttribute(&P.num_sms, cudaDevAttrMultiProcessorCount, dev);
+  std::vector<visar_stage> st(stages, stages + nstages);
+
+  // Pass 1 sizes the pool (inputs owned by the plan, outputs, tables,
+  // descriptors); pass 2 builds the plan inside it.
+  P.inputs.resize(n);
+  Builder sizing{P, true, {}, {}};
+  for (size_t i = 0; i < n; i++) {
+    const visar_image &c = inputs[i];
+    if (c.data) P.inputs[i] = Buf{DImg{static_cast<uint8_t *>(c.data), (long long)c.stride, (int)c.width, (int)c.height, (int)c.channels}, (int)c.depth};
+    else sizing.image((int)c.width, (int)c.height, (int)c.channels, (int)c.depth, P.inputs[i]);
+  }
+  int rc = build_all(sizing, st);
+  if (rc != VISAR_OK) return report_error(rc, rc == VISAR_UNSUPPORTED ? "Unsupported" : "InvalidArgument");
+  size_t desc_bytes = 0;
+  int nl = 0;
+  for (const Step &s : P.steps)
+    for (const Launch &L : s.launches) {
+      desc_bytes += ((sizeof(BImg) * L.imgs.size() + 255) & ~(size_t)255) + ((sizeof(int) * (L.imgs.size() + 1) + 255) & ~(size_t)255);
+      nl++;
+    }
+  const size_t total = sizing.sz.bytes + desc_bytes + sizeof(int) * (size_t)(nl + 1) + 4096;
+  e = cudaMalloc(&P.pool.base, total);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return report_error(VISAR_OUT_OF_MEMORY, "OutOfMemory");
+  }
+  P.pool.cap = total;
+  Builder B{P, false, {}, {}};
+  for (size_t i = 0; i < n; i++)
+    if (!inputs[i].data && !B.image((int)inputs[i].width, (int)inputs[i].height, (int)inputs[i].channels, (int)inputs[i].depth, P.inputs[i]))
+      return report_error(VISAR_OUT_OF_MEMORY, "OutOfMemory");
+  rc = build_all(B, st);
+  if (rc != VISAR_OK) return report_error(rc, rc == VISAR_OUT_OF_MEMORY ? "OutOfMemory" : "InvalidArgument");
+  // Descriptors and prefix sums of every launch.
+  P.ncounters = 0;
+  for (Step &s : P.steps) {
+    for (Launch &L : s.launches) {
+      std::vector<int> start(L.imgs.size() + 1, 0);
+      for (size_t i = 0; i < L.imgs.size(); i++) start[i + 1] = start[i] + L.imgs[i].tiles_x * L.imgs[i].tiles_y;
+      L.total = start.back();
+      L.d_imgs = B.table(L.imgs);
+      L.d_start = B.table(start);
+      if (!L.d_imgs || !L.d_start) return report_error(VISAR_OUT_OF_MEMORY, "OutOfMemory");
+      L.counter = P.ncounters++;
+      P.bytes += L.bytes;
+      P.nlaunch++;
+    }
+    P.nfallback += s.fallbacks.size();
+    for (const Fallback &f : s.fallbacks)
+      P.bytes += ((size_t)f.s.v.w * f.s.v.h * f.s.v.cn + (size_t)f.d.v.w * f.d.v.h * f.d.v.cn) * (size_t)depth_size(f.s.depth);
+  }
+  P.counters = static_cast<int *>(P.pool.take(sizeof(int) * (size_t)std::max(1, P.ncounters)));
+  if (!P.counters) return report_error(VISAR_OUT_OF_MEMORY, "OutOfMemory");
+  for (const Builder::Upload &u : B.uploads) {
+    e = cudaMemcpy(u.dst, u.data.data(), u.data.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_status(e);
+  }
+  for (size_t i = 0; i < n; i++) P.pixels_in += (size_t)inputs[i].width * inputs[i].height;
+  e = cudaStreamCreateWithFlags(&P.own, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return cuda_status(e);
+  *out = b.release();
+  return VISAR_OK;
+}
+
+int visar_batch_input(const visar_batch *b, size_t i, visar_image *out) {
+  if (!b || !out || i >= b->plan.inputs.size()) return report_error(VISAR_INVALID_ARGUMENT, "InvalidArgument");
+  *out = cimg(b->plan.inputs[i]);
+  return VISAR_OK;
+}
+
+int visar_batch_stage_output(const visar_batch *b, size_t stage, size_t i, visar_image *out) {
+  if (!b || !out || stage >= b->plan.outs.size() || i >= b->plan.inputs.size())
+    return report_error(VISAR_INVALID_ARGUMENT, "InvalidArgument");
+  *out = cimg(b->plan.outs[stage][i]);
+  return VISAR_OK;
+}
+
+int visar_batch_output(const visar_batch *b, size_t i, visar_image *out) {
+  if (!b || !out || i >= b->plan.inputs.size()) return report_error(VISAR_INVALID_ARGUMENT, "InvalidArgument");
+  *out = cimg(b->plan.outs.empty() ? b->plan.inputs[i] : b->plan.outs.back()[i]);
+  return VISAR_OK;
+}
+
+int visar_batch_run(visar_batch *b) {
+  if (!b) return report_error(VISAR_INVALID_ARGUMENT, "InvalidArgument");
+  Plan &P = b->plan;
+  cudaError_t e = cudaSetDevice(P.dev);
+  if (e != cudaSuccess) return cuda_status(e);
+  const cudaStream_t st = run_stream(P);
+  const int rc = enqueue(P, st);
+  if (rc != VISAR_OK) return rc;
+  return finish(st);
+}
+
+int visar_batch_run_graph(visar_batch *b) {
+  if (!b) return report_error(VISAR_INVALID_ARGUMENT, "InvalidArgument");
+  Plan &P = b->plan;
+  if (P.nfallback > 0) return visar_batch_run(b);
+  cudaError_t e = cudaSetDevice(P.dev);
+  if (e != cudaSuccess) return cuda_status(e);
+  const cudaStream_t st = run_stream(P);
+  if (!P.graph) {
+    // Capture on the plan's own stream (never the legacy default stream).
+    e = cudaStreamBeginCapture(P.own, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return cuda_status(e);
+    const int rc = enqueue(P, P.own);
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(P.own, &g);
+    if (rc != VISAR_OK) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (e != cudaSuccess) return cuda_status(e);
+    e = cudaGraphInstantiate(&P.graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+      P.graph = nullptr;
+      return cuda_status(e);
+    }
+  }
+  e = cudaGraphLaunch(P.graph, st);
+  if (e != cudaSuccess) return cuda_status(e);
+  return finish(st);
+}
+
+int visar_batch_get_info(const visar_batch *b, visar_batch_info *info) {
+  if (!b || !info) return report_error(VISAR_INVALID_ARGUMENT, "InvalidArgument");
+  const Plan &P = b->plan;
+  info->images = P.inputs.size();
+  info->stages = P.steps.size();
+  info->launches = P.nlaunch;
+  info->fallback_calls = P.nfallback;
+  info->pool_bytes = P.pool.cap;
+  info->bytes_moved = P.bytes;
+  info->pixels_in = P.pixels_in;
+  return VISAR_OK;
+}
+
+void visar_batch_destroy(visar_batch *b) {
+  if (!b) return;
+  cudaSetDevice(b->plan.dev);
+  cudaStreamSynchronize(b->plan.own);
+  delete b;
+}
+
+int visar_tune_load(const char *path) {
+  std::map<std::string, int> m;
+  if (path) {
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return report_error(VISAR_INVALID_ARGUMENT, "InvalidArgument: tuning file not readable");
+    std::string txt;
+    char buf[4096];
+    size_t k;
+    while ((k = std::fread(buf, 1, sizeof(buf), f)) > 0) txt.append(buf, k);
+    std::fclose(f);
+    if (!parse_tune_json(txt, m)) return report_error(VISAR_INVALID_DATA, "InvalidData: tuning file");
+  }
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune = std::move(m);
+  return VISAR_OK;
+}
+
+int visar_tune_set(const char *key, int value) {
+  if (!key) return report_error(VISAR_INVALID_ARGUMENT, "InvalidArgument");
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune[key] = value;
+  return VISAR_OK;
+}
+
+int visar_tune_get(const char *key, int fallback) {
+  if (!key) return fallback;
+  return tune_get(key, fallback);
+}
+
+}  // extern "C"

@@ -516,6 +516,18 @@ std::vector<MorphRun> element_runs(const std::vector<uint8_t> &m, int w, int h) 
 
 void note_launch(int n) { g_launches.fetch_add((unsigned long long)n, std::memory_order_relaxed); }
 
+cudaStream_t thread_stream() { return t_stream; }
+int thread_async() { return t_async; }
+void set_thread_stream(cudaStream_t st, int async) {
+  t_stream = st;
+  t_async = async;
+}
+
+int report_error(int status, const char *msg) {
+  set_error(msg);
+  return status;
+}
+
 }  // namespace vb
 
 using namespace vb;
@@ -964,15 +976,9 @@ int visar_warp_affine(const visar_image *src, const visar_image *dst, const doub
     std::lock_guard<std::mutex> lk(g_mu);
     View s = typed(src, depth);
     View d = typed(dst, depth);
-    // invertAffine (geometry.zig:591-602), then rounded to f32 (geometry.zig:412-415)
-    const double det = m[0] * m[4] - m[1] * m[3];
-    if (det == 0) unsupported();
+    float mf[6];
+    if (!affine_inverse_f32(m, mf)) unsupported();
     if (s.c->channels != d.c->channels) size_mismatch();
-    const double dd = 1.0 / det;
-    const double a11 = m[4] * dd, a22 = m[0] * dd, a12 = -m[1] * dd, a21 = -m[3] * dd;
-    const double b1 = -a11 * m[2] - a12 * m[5];
-    const double b2 = -a21 * m[2] - a22 * m[5];
-    const float mf[6] = {(float)a11, (float)a12, (float)b1, (float)a21, (float)a22, (float)b2};
     Call call = begin_call();
     stage_in(call, s, kSrc);
     stage_out(call, d, kDst);
@@ -992,16 +998,9 @@ int visar_warp_perspective(const visar_image *src, const visar_image *dst, const
     std::lock_guard<std::mutex> lk(g_mu);
     View s = typed(src, depth);
     View d = typed(dst, depth);
-    // invert3 (geometry.zig:604-613)
-    const double det = m[0] * (m[4] * m[8] - m[5] * m[7]) - m[1] * (m[3] * m[8] - m[5] * m[6]) + m[2] * (m[3] * m[7] - m[4] * m[6]);
-    if (det == 0) unsupported();
+    double inv[9];
+    if (!perspective_inverse(m, inv)) unsupported();
     if (s.c->channels != d.c->channels) size_mismatch();
-    const double r = 1.0 / det;
-    const double inv[9] = {
-        (m[4] * m[8] - m[5] * m[7]) * r, (m[2] * m[7] - m[1] * m[8]) * r, (m[1] * m[5] - m[2] * m[4]) * r,
-        (m[5] * m[6] - m[3] * m[8]) * r, (m[0] * m[8] - m[2] * m[6]) * r, (m[2] * m[3] - m[0] * m[5]) * r,
-        (m[3] * m[7] - m[4] * m[6]) * r, (m[1] * m[6] - m[0] * m[7]) * r, (m[0] * m[4] - m[1] * m[3]) * r,
-    };
     Call call = begin_call();
     stage_in(call, s, kSrc);
     stage_out(call, d, kDst);

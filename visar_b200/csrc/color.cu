@@ -8,7 +8,6 @@ namespace vb {
 
 namespace {
 
-constexpr int kGrayShift = 15, kB2G = 3735, kG2G = 19235, kR2G = 9798;
 constexpr int kYShift = 14, kR2Y = 4899, kG2Y = 9617, kB2Y = 1868;
 constexpr int kHsvShift = 12;
 

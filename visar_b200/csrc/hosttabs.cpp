@@ -79,4 +79,40 @@ std::vector<uint8_t> structuring_element(int shape, int w, int h) {
   return m;
 }
 
+// invertAffine (src/imgproc/geometry.zig:591-602) in f64, rounded to f32 as
+// warpAffine uses it (geometry.zig:412-415). False for a singular matrix.
+bool affine_inverse_f32(const double m[6], float out[6]) {
+  const double det = m[0] * m[4] - m[1] * m[3];
+  if (det == 0) return false;
+  const double dd = 1.0 / det;
+  const double a11 = m[4] * dd, a22 = m[0] * dd, a12 = -m[1] * dd, a21 = -m[3] * dd;
+  const double b1 = -a11 * m[2] - a12 * m[5];
+  const double b2 = -a21 * m[2] - a22 * m[5];
+  out[0] = (float)a11;
+  out[1] = (float)a12;
+  out[2] = (float)b1;
+  out[3] = (float)a21;
+  out[4] = (float)a22;
+  out[5] = (float)b2;
+  return true;
+}
+
+// invert3 (src/imgproc/geometry.zig:604-613): adjugate over the determinant.
+bool perspective_inverse(const double m[9], double out[9]) {
+  const double det = m[0] * (m[4] * m[8] - m[5] * m[7]) - m[1] * (m[3] * m[8] - m[5] * m[6]) +
+                     m[2] * (m[3] * m[7] - m[4] * m[6]);
+  if (det == 0) return false;
+  const double r = 1.0 / det;
+  out[0] = (m[4] * m[8] - m[5] * m[7]) * r;
+  out[1] = (m[2] * m[7] - m[1] * m[8]) * r;
+  out[2] = (m[1] * m[5] - m[2] * m[4]) * r;
+  out[3] = (m[5] * m[6] - m[3] * m[8]) * r;
+  out[4] = (m[0] * m[8] - m[2] * m[6]) * r;
+  out[5] = (m[2] * m[3] - m[0] * m[5]) * r;
+  out[6] = (m[3] * m[7] - m[4] * m[6]) * r;
+  out[7] = (m[1] * m[6] - m[0] * m[7]) * r;
+  out[8] = (m[0] * m[4] - m[1] * m[3]) * r;
+  return true;
+}
+
 }  // namespace vb

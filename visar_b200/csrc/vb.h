@@ -17,6 +17,12 @@ inline int depth_size(int d) { return d == k8U ? 1 : (d == k16U || d == k16S) ? 
 
 // Counts kernel launches made by the library (reported by visar_cuda_launch_count).
 void note_launch(int n = 1);
+// The calling thread's stream and async flag (visar_cuda_set_stream / _async).
+cudaStream_t thread_stream();
+int thread_async();
+void set_thread_stream(cudaStream_t st, int async);
+// Records `msg` as the thread's last error and returns `status`.
+int report_error(int status, const char *msg);
 
 // ------------------------------------------------------------- color
 // Conversion kinds of src/imgproc/color.zig:44-46.
@@ -26,6 +32,8 @@ struct ColorInfo {
   ColorKind kind;
 };
 cudaError_t launch_cvt_color(const DImg &s, const DImg &d, int depth, const ColorInfo &ci, cudaStream_t st);
+// RGB -> gray in 15-bit fixed point (src/imgproc/color.zig:120-130, 8- and 16-bit).
+constexpr int kGrayShift = 15, kB2G = 3735, kG2G = 19235, kR2G = 9798;
 
 // ---------------------------------------------------- separable filter
 // Finishing step of a separable filter (src/imgproc/filter.zig:60-116).
@@ -112,6 +120,9 @@ int sat_i16(float x);
 LinTap lin_tap_u8(long long d, uint32_t ssize, uint32_t dsize, bool area, bool pin);
 // getStructuringElement (src/imgproc/morph.zig:32-59): h x w mask, row-major.
 std::vector<uint8_t> structuring_element(int shape, int w, int h);
+// warpAffine's inverse map in f32 / warpPerspective's in f64; false if singular.
+bool affine_inverse_f32(const double m[6], float out[6]);
+bool perspective_inverse(const double m[9], double out[9]);
 
 // ------------------------------------- resize with a static tap buffer
 // Largest destination width or height of the allocation-free linear resize.

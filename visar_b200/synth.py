@@ -80,3 +80,37 @@ def perspective_params(w, h, seed, jitter=80.0):
     src = [(0.0, 0.0), (w - 1.0, 0.0), (w - 1.0, h - 1.0), (0.0, h - 1.0)]
     dst = [(x + rng.uniform(-jitter, jitter), y + rng.uniform(-jitter, jitter)) for x, y in src]
     return homography_from_corners(src, dst)
+
+
+def mixed_shapes(n=256, seed=2, wmin=64, wmax=4096, hmin=64, hmax=2160, channels=(1, 3)):
+    """(height, width, channels) of the mixed-size batch: uniform integer sides, channels drawn uniformly."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        w = int(rng.integers(wmin, wmax + 1))
+        h = int(rng.integers(hmin, hmax + 1))
+        c = int(channels[int(rng.integers(0, len(channels)))])
+        out.append((h, w, c))
+    return out
+
+
+def base_image_torch(h, w, c=3, nrect=8, seed=0, device="cuda"):
+    """base_image's recipe generated on the device (for large batches); a uint8 torch tensor."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(int(seed))
+    x = torch.arange(w, device=device, dtype=torch.float64)
+    grad = torch.round(x * 255.0 / max(w - 1, 1)).to(torch.int32)
+    noise = torch.randint(-20, 21, (h, w, c), generator=g, device=device, dtype=torch.int32)
+    img = (grad[None, :, None] + noise).clamp_(0, 255).to(torch.uint8)
+    rng = np.random.default_rng(seed)
+    for _ in range(nrect):
+        rw = int(rng.integers(20, 161))
+        rh = int(rng.integers(20, 161))
+        x0 = int(rng.integers(0, max(1, w - rw + 1)))
+        y0 = int(rng.integers(0, max(1, h - rh + 1)))
+        col = torch.as_tensor(rng.integers(0, 256, size=c).astype(np.uint8), device=device)
+        img[y0:y0 + rh, x0:x0 + rw] = col
+    if c == 1:
+        img = img[:, :, 0]
+    return img.contiguous()
