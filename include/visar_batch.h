@@ -87,6 +87,33 @@ int visar_batch_run_graph(visar_batch *b);
 int visar_batch_get_info(const visar_batch *b, visar_batch_info *info);
 void visar_batch_destroy(visar_batch *b);
 
+/* Points input i at another device image of the same width, height,
+   channels, depth, row stride and at least the same alignment (e.g. the next
+   video frame). Enqueued on the run stream (a one-thread kernel patches the
+   device descriptors), so graph replays see it. */
+int visar_batch_set_input(visar_batch *b, size_t i, const visar_image *img);
+/* Host <-> device copies of all inputs / final outputs (one 2-D copy per
+   image, from or to `host[i]`, which must match the image's shape; pinned
+   host memory keeps them asynchronous). Same stream and async rules as
+   visar_batch_run. */
+int visar_batch_upload(visar_batch *b, const visar_image *host, size_t n);
+int visar_batch_download(visar_batch *b, const visar_image *host, size_t n);
+
+/* Per-launch timing: with profiling on, eager runs (visar_batch_run) record
+   a CUDA event pair around every persistent launch on the run stream. */
+typedef struct visar_batch_launch_stat {
+    char name[48];          /* op.depth.channels.kernel (e.g. "gauss.u8.c1.k5") */
+    int stage;
+    size_t images;
+    size_t tiles;
+    size_t bytes;           /* algorithmic bytes of the launch */
+    int grid;               /* CTAs launched */
+    float ms;               /* duration in the last profiled run (0 if none) */
+} visar_batch_launch_stat;
+
+int visar_batch_profile(visar_batch *b, int enable);
+int visar_batch_launch_stat_get(const visar_batch *b, size_t i, visar_batch_launch_stat *out);
+
 /* Tuning table (written by the autotuner, visar_b200/autotune.py): a flat
    JSON object of "key": integer entries. NULL restores the built-in defaults.
    Plans built afterwards use it. */

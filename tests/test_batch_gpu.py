@@ -185,3 +185,34 @@ def test_tuning_choices_give_identical_results():
                 check_plan(imgs, C2 + [("thresh", {"t": 128, "m": 255, "type": 0})])
     finally:
         B.tune_load(None)
+
+
+def test_rebind_upload_download_and_profile():
+    imgs = mixed_u8(6, seed=41, wmax=700, hmax=400)
+    plan = B.Batch([(x.shape[0], x.shape[1], 1 if x.ndim == 2 else x.shape[2], np.uint8) for x in imgs],
+                   [batch_stage(s) for s in C2])
+    hosts = [torch.empty(tuple(x.shape), dtype=torch.uint8, pin_memory=True).numpy() for x in imgs]
+    for h, x in zip(hosts, imgs):
+        h[...] = x.cpu().numpy()
+    plan.upload(hosts)
+    plan.profile(True)
+    check_plan(imgs, C2, plan=plan)
+    stats = plan.launch_stats()
+    assert len(stats) == plan.info()["launches"] and all(s["ms"] > 0 and s["grid"] > 0 for s in stats)
+    assert sum(s["bytes"] for s in stats) == plan.info()["bytes_moved"]
+    outs = [np.empty(tuple(plan.output(i).shape), np.uint8) for i in range(len(imgs))]
+    plan.download(outs)
+    for i, o in enumerate(outs):
+        assert np.array_equal(o, plan.output(i).cpu().numpy())
+    # Rebind input 0 to another device image with the plan input's row pitch.
+    x0 = imgs[0]
+    c0 = 1 if x0.ndim == 2 else x0.shape[2]
+    new0 = synth.base_image_torch(x0.shape[0], x0.shape[1], c0, nrect=5, seed=999)
+    pitch = plan.input(0).stride(0)
+    big = torch.zeros((new0.shape[0], pitch), dtype=torch.uint8, device="cuda")
+    view = big[:, :new0.shape[1] * c0]
+    view.copy_(new0.reshape(new0.shape[0], -1))
+    if c0 > 1:
+        view = view.view(new0.shape[0], new0.shape[1], c0)
+    plan.set_input(0, view)
+    check_plan([new0] + imgs[1:], C2, graph=True, plan=plan)

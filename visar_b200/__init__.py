@@ -45,7 +45,7 @@ class Image(ctypes.Structure):
 
 def _load():
     if not os.path.exists(LIB_PATH):
-        raise ImportError(f"visar_b200: CUDA library not built ({LIB_PATH}); run `python -m visar_b200.build`")
+        raise ImportError(f"visar_b200: CUDA library not built ({LIB_PATH}); run `python visar_b200/build.py`")
     lib = ctypes.CDLL(LIB_PATH)
     lib.visar_version.restype = ctypes.c_char_p
     lib.visar_build_info.restype = ctypes.c_char_p

@@ -44,6 +44,18 @@ lib.visar_batch_run_graph.argtypes = [ctypes.c_void_p]
 lib.visar_batch_get_info.argtypes = [ctypes.c_void_p, ctypes.POINTER(BatchInfo)]
 lib.visar_batch_destroy.argtypes = [ctypes.c_void_p]
 lib.visar_batch_destroy.restype = None
+lib.visar_batch_set_input.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.POINTER(Image)]
+lib.visar_batch_upload.argtypes = [ctypes.c_void_p, ctypes.POINTER(Image), ctypes.c_size_t]
+lib.visar_batch_download.argtypes = [ctypes.c_void_p, ctypes.POINTER(Image), ctypes.c_size_t]
+lib.visar_batch_profile.argtypes = [ctypes.c_void_p, ctypes.c_int]
+
+
+class LaunchStat(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 48), ("stage", ctypes.c_int), ("images", ctypes.c_size_t),
+                ("tiles", ctypes.c_size_t), ("bytes", ctypes.c_size_t), ("grid", ctypes.c_int), ("ms", ctypes.c_float)]
+
+
+lib.visar_batch_launch_stat_get.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.POINTER(LaunchStat)]
 lib.visar_tune_load.argtypes = [ctypes.c_char_p]
 lib.visar_tune_set.argtypes = [ctypes.c_char_p, ctypes.c_int]
 lib.visar_tune_get.argtypes = [ctypes.c_char_p, ctypes.c_int]
@@ -166,6 +178,33 @@ class Batch:
         img = Image()
         _check(lib.visar_batch_output(self._h, i, ctypes.byref(img)))
         return _as_tensor(img, self)
+
+    def set_input(self, i, x):
+        """Rebinds input i to device tensor x (same shape, dtype, row stride and alignment)."""
+        self._keep.append(x)
+        _check(lib.visar_batch_set_input(self._h, i, ctypes.byref(desc(x))))
+
+    def upload(self, hosts):
+        """Host -> device copy of every input from NumPy arrays (pinned for asynchrony)."""
+        arr = (Image * len(hosts))(*[desc(h) for h in hosts])
+        _check(lib.visar_batch_upload(self._h, arr, len(hosts)))
+
+    def download(self, hosts):
+        """Device -> host copy of every final output into NumPy arrays."""
+        arr = (Image * len(hosts))(*[desc(h) for h in hosts])
+        _check(lib.visar_batch_download(self._h, arr, len(hosts)))
+
+    def profile(self, enable=True):
+        _check(lib.visar_batch_profile(self._h, int(bool(enable))))
+
+    def launch_stats(self):
+        out = []
+        for i in range(self.info()["launches"]):
+            st = LaunchStat()
+            _check(lib.visar_batch_launch_stat_get(self._h, i, ctypes.byref(st)))
+            out.append({"name": st.name.decode(), "stage": st.stage, "images": st.images, "tiles": st.tiles,
+                        "bytes": st.bytes, "grid": st.grid, "ms": st.ms})
+        return out
 
     def stage_output(self, stage, i):
         img = Image()

@@ -4,7 +4,7 @@ Device code is compiled with --fmad=false so that no multiply-add is fused
 unless the source asks for it (fmaf/fma), which keeps f32 results in VISAR's
 operation order; host code gets -ffp-contract=off for the same reason.
 
-Usage: python -m visar_b200.build [--force]
+Usage: python visar_b200/build.py [--force]   (the package import needs the built library)
 """
 import os
 import subprocess

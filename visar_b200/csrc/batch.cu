@@ -68,6 +68,7 @@ bool parse_tune_json(const std::string &txt, std::map<std::string, int> &out) {
 struct Buf {
   DImg v;
   int depth;
+  int input = -1;  // index of the plan input this buffer is, else -1
 };
 
 enum OpKind { kOpGauss, kOpMorph, kOpGray, kOpHalf, kOpLinear, kOpLut, kOpWarpAff, kOpWarpPer };
@@ -100,7 +101,10 @@ struct Launch {
   WarpArgs wa{};
   const uint8_t *lut = nullptr;
   std::vector<BImg> imgs;
+  std::vector<int> src_input;  // per image: the plan input it reads, else -1
   size_t bytes = 0;  // algorithmic bytes
+  int stage = 0;
+  mutable int grid = 0;
   BImg *d_imgs = nullptr;
   int *d_start = nullptr;
   int total = 0;
@@ -145,7 +149,11 @@ struct Plan {
   size_t pixels_in = 0, bytes = 0, nlaunch = 0, nfallback = 0;
   cudaStream_t own = nullptr;
   cudaGraphExec_t graph = nullptr;
+  bool prof = false;
+  bool prof_valid = false;
+  std::vector<cudaEvent_t> evs;  // 2 per launch when profiling
   ~Plan() {
+    for (cudaEvent_t e : evs) cudaEventDestroy(e);
     if (graph) cudaGraphExecDestroy(graph);
     if (pool.base) cudaFree(pool.base);
     if (own) cudaStreamDestroy(own);
@@ -214,6 +222,11 @@ std::string launch_key(const Launch &L) {
   char buf[96];
   std::snprintf(buf, sizeof(buf), "%s.%s.c%d.k%d", op_name(L.op), L.depth == k32F ? "f32" : "u8", L.cn, L.k);
   return buf;
+}
+
+const char *launch_suffix(const Launch &L) {
+  if (L.op != kOpMorph) return "";
+  return L.is_max ? ".max" : ".min";
 }
 
 Launch *class_of(std::vector<Launch> &ls, int op, int depth, int cn, int k, bool is_max) {
@@ -301,6 +314,11 @@ BImg bimg(const DImg &s, const DImg &d) {
   return b;
 }
 
+void add_img(Launch *l, const BImg &b, int input) {
+  l->imgs.push_back(b);
+  l->src_input.push_back(input);
+}
+
 void u8_bytes(Launch &L, const DImg &s, const DImg &d, int esize) {
   L.bytes += ((size_t)s.w * s.h * s.cn + (size_t)d.w * d.h * d.cn) * (size_t)esize;
 }
@@ -337,7 +355,7 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
           continue;
         }
         Launch *l = class_of(ls, kOpGray, k8U, im.v.cn, 0, false);
-        l->imgs.push_back(bimg(im.v, next[i].v));
+        add_img(l, bimg(im.v, next[i].v), im.input);
         u8_bytes(*l, im.v, next[i].v, 1);
       }
       break;
@@ -388,7 +406,7 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
         }
         Launch *l = class_of(ls, kOpGauss, im.depth, im.v.cn, kw, false);
         l->fa = a;
-        l->imgs.push_back(bimg(im.v, next[i].v));
+        add_img(l, bimg(im.v, next[i].v), im.input);
         u8_bytes(*l, im.v, next[i].v, depth_size(im.depth));
       }
       break;
@@ -435,7 +453,7 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
           const DImg dst = p + 1 == np ? next[i].v : tmp[i][p % 2].v;
           Launch *l = class_of(pl, kOpMorph, k8U, im.v.cn, kh, passes[p]);
           fast::morph_fast_args(mask, kw, kh, im.v.cn, im.v.w, l->ma);
-          l->imgs.push_back(bimg(src, dst));
+          add_img(l, bimg(src, dst), p == 0 ? im.input : -1);
           u8_bytes(*l, src, dst, 1);
         }
         for (Launch &l : pl) {
@@ -468,7 +486,7 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
         }
         if (im.v.w == 2 * dw && im.v.h == 2 * dh) {
           Launch *l = class_of(ls, kOpHalf, k8U, im.v.cn, 0, false);
-          l->imgs.push_back(bimg(im.v, next[i].v));
+          add_img(l, bimg(im.v, next[i].v), im.input);
           u8_bytes(*l, im.v, next[i].v, 1);
         } else {
           std::vector<LinTap> xt(dw), yt(dh);
@@ -479,7 +497,7 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
           b.t1 = B.table(yt);
           if (!B.sizing && (!b.t0 || !b.t1)) return VISAR_OUT_OF_MEMORY;
           Launch *l = class_of(ls, kOpLinear, k8U, im.v.cn, 0, false);
-          l->imgs.push_back(b);
+          add_img(l, b, im.input);
           u8_bytes(*l, im.v, next[i].v, 1);
         }
       }
@@ -521,7 +539,7 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
         }
         Launch *l = class_of(ls, kOpLut, k8U, 0, 0, false);
         l->lut = dlut;
-        l->imgs.push_back(bimg(im.v, next[i].v));
+        add_img(l, bimg(im.v, next[i].v), im.input);
         u8_bytes(*l, im.v, next[i].v, 1);
       }
       break;
@@ -555,7 +573,7 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
         b.wide = ((uintptr_t)im.v.p % 8 == 0) && (im.v.stride % 8 == 0);
         Launch *l = class_of(ls, persp ? kOpWarpPer : kOpWarpAff, im.depth, im.v.cn, 0, false);
         l->wa = WarpArgs{interp, border};
-        l->imgs.push_back(b);
+        add_img(l, b, im.input);
         u8_bytes(*l, im.v, next[i].v, depth_size(im.depth));
       }
       break;
@@ -580,6 +598,7 @@ int build_all(Builder &B, const std::vector<visar_stage> &stages) {
     std::vector<Buf> next;
     const int rc = build_stage(B, st, cur, next, step);
     if (rc != VISAR_OK) return rc;
+    for (Launch &l : step.launches) l.stage = (int)P.steps.size();
     P.steps.push_back(std::move(step));
     P.outs.push_back(next);
     cur = next;
@@ -613,6 +632,7 @@ cudaError_t run_op(const Plan &P, const Launch &L, const typename Op::Args &a, c
   }
   const int per_sm = L.per_sm > 0 ? std::min(L.per_sm, std::max(occ, 1)) : std::max(occ, 1);
   const int grid = std::max(1, std::min(L.total, P.num_sms * per_sm));
+  L.grid = grid;
   kern<<<grid, Op::kThreads, smem, st>>>(q, a);
   note_launch();
   return cudaGetLastError();
@@ -740,15 +760,19 @@ int cuda_status(cudaError_t e) {
 }
 
 // Enqueues the whole plan on st. Fallback calls run on st in async mode.
-int enqueue(Plan &P, cudaStream_t st) {
+int enqueue(Plan &P, cudaStream_t st, bool timed) {
   if (P.ncounters > 0) {
     const cudaError_t e = cudaMemsetAsync(P.counters, 0, sizeof(int) * (size_t)P.ncounters, st);
     if (e != cudaSuccess) return cuda_status(e);
   }
+  size_t j = 0;
   for (const Step &s : P.steps) {
     for (const Launch &L : s.launches) {
+      if (timed) cudaEventRecord(P.evs[2 * j], st);
       const cudaError_t e = run_launch(P, L, st);
       if (e != cudaSuccess) return cuda_status(e);
+      if (timed) cudaEventRecord(P.evs[2 * j + 1], st);
+      j++;
     }
     if (!s.fallbacks.empty()) {
       const cudaStream_t old = thread_stream();
@@ -764,6 +788,14 @@ int enqueue(Plan &P, cudaStream_t st) {
     }
   }
   return VISAR_OK;
+}
+
+// Points the source of descriptor j at p (input rebinding).
+__global__ void k_patch_src(BImg *imgs, int j, uint8_t *p) { imgs[j].s.p = p; }
+
+bool same_shape(const visar_image &c, const Buf &b) {
+  return c.width == (uint32_t)b.v.w && c.height == (uint32_t)b.v.h && c.channels == (uint32_t)b.v.cn &&
+         c.depth == (uint32_t)b.depth;
 }
 
 cudaStream_t run_stream(Plan &P) {
@@ -831,6 +863,7 @@ int visar_batch_create(const visar_image *inputs, size_t n, const visar_stage *s
     const visar_image &c = inputs[i];
     if (c.data) P.inputs[i] = Buf{DImg{static_cast<uint8_t *>(c.data), (long long)c.stride, (int)c.width, (int)c.height, (int)c.channels}, (int)c.depth};
     else sizing.image((int)c.width, (int)c.height, (int)c.channels, (int)c.depth, P.inputs[i]);
+    P.inputs[i].input = (int)i;
   }
   int rc = build_all(sizing, st);
   if (rc != VISAR_OK) return report_error(rc, rc == VISAR_UNSUPPORTED ? "Unsupported" : "InvalidArgument");
@@ -849,9 +882,11 @@ int visar_batch_create(const visar_image *inputs, size_t n, const visar_stage *s
   }
   P.pool.cap = total;
   Builder B{P, false, {}, {}};
-  for (size_t i = 0; i < n; i++)
+  for (size_t i = 0; i < n; i++) {
     if (!inputs[i].data && !B.image((int)inputs[i].width, (int)inputs[i].height, (int)inputs[i].channels, (int)inputs[i].depth, P.inputs[i]))
       return report_error(VISAR_OUT_OF_MEMORY, "OutOfMemory");
+    P.inputs[i].input = (int)i;
+  }
   rc = build_all(B, st);
   if (rc != VISAR_OK) return report_error(rc, rc == VISAR_OUT_OF_MEMORY ? "OutOfMemory" : "InvalidArgument");
   // Descriptors and prefix sums of every launch.
@@ -910,8 +945,10 @@ int visar_batch_run(visar_batch *b) {
   cudaError_t e = cudaSetDevice(P.dev);
   if (e != cudaSuccess) return cuda_status(e);
   const cudaStream_t st = run_stream(P);
-  const int rc = enqueue(P, st);
+  const bool timed = P.prof && P.evs.size() == 2 * P.nlaunch;
+  const int rc = enqueue(P, st, timed);
   if (rc != VISAR_OK) return rc;
+  P.prof_valid = timed;
   return finish(st);
 }
 
@@ -926,7 +963,7 @@ int visar_batch_run_graph(visar_batch *b) {
     // Capture on the plan's own stream (never the legacy default stream).
     e = cudaStreamBeginCapture(P.own, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return cuda_status(e);
-    const int rc = enqueue(P, P.own);
+    const int rc = enqueue(P, P.own, false);
     cudaGraph_t g = nullptr;
     e = cudaStreamEndCapture(P.own, &g);
     if (rc != VISAR_OK) {
@@ -964,6 +1001,119 @@ void visar_batch_destroy(visar_batch *b) {
   cudaSetDevice(b->plan.dev);
   cudaStreamSynchronize(b->plan.own);
   delete b;
+}
+
+int visar_batch_set_input(visar_batch *b, size_t i, const visar_image *img) {
+  if (!b || !img || !img->data || i >= b->plan.inputs.size()) return report_error(VISAR_INVALID_ARGUMENT, "InvalidArgument");
+  Plan &P = b->plan;
+  if (!same_shape(*img, P.inputs[i])) return report_error(VISAR_SIZE_MISMATCH, "SizeMismatch");
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, img->data) != cudaSuccess ||
+      !(a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) || a.device != P.dev) {
+    cudaGetLastError();
+    return report_error(VISAR_INVALID_ARGUMENT, "InvalidArgument: batch inputs must be device memory of the plan's device");
+  }
+  uint8_t *np = static_cast<uint8_t *>(img->data);
+  const long long nstride = (long long)img->stride;
+  // Kernel choices depend on the source layout; a new pointer must keep it.
+  const uint8_t *op = P.inputs[i].v.p;
+  const long long ostride = P.inputs[i].v.stride;
+  if (nstride != ostride) return report_error(VISAR_INVALID_ARGUMENT, "InvalidArgument: rebound input has another stride");
+  for (int al : {16, 8, 4})
+    if ((uintptr_t)op % al == 0 && (uintptr_t)np % al != 0)
+      return report_error(VISAR_INVALID_ARGUMENT, "InvalidArgument: rebound input is less aligned than the original");
+  cudaError_t e = cudaSetDevice(P.dev);
+  if (e != cudaSuccess) return cuda_status(e);
+  const cudaStream_t st = run_stream(P);
+  for (Step &s : P.steps) {
+    for (Launch &L : s.launches)
+      for (size_t j = 0; j < L.imgs.size(); j++)
+        if (L.src_input[j] == (int)i) {
+          L.imgs[j].s.p = np;
+          k_patch_src<<<1, 1, 0, st>>>(L.d_imgs, (int)j, np);
+          note_launch();
+          e = cudaGetLastError();
+          if (e != cudaSuccess) return cuda_status(e);
+        }
+    for (Fallback &f : s.fallbacks)
+      if (f.s.input == (int)i) f.s.v.p = np;
+  }
+  for (auto &stage : P.outs)
+    if (stage[i].input == (int)i) stage[i].v.p = np;  // pass-through stages
+  P.inputs[i].v.p = np;
+  return finish(st);
+}
+
+int visar_batch_upload(visar_batch *b, const visar_image *host, size_t n) {
+  if (!b || (n > 0 && !host) || n != b->plan.inputs.size()) return report_error(VISAR_INVALID_ARGUMENT, "InvalidArgument");
+  Plan &P = b->plan;
+  cudaError_t e = cudaSetDevice(P.dev);
+  if (e != cudaSuccess) return cuda_status(e);
+  const cudaStream_t st = run_stream(P);
+  for (size_t i = 0; i < n; i++) {
+    const Buf &d = P.inputs[i];
+    if (!host[i].data || !same_shape(host[i], d)) return report_error(VISAR_SIZE_MISMATCH, "SizeMismatch");
+    const size_t rb = (size_t)d.v.w * d.v.cn * depth_size(d.depth);
+    e = cudaMemcpy2DAsync(d.v.p, (size_t)d.v.stride, host[i].data, host[i].stride, rb, (size_t)d.v.h, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return cuda_status(e);
+  }
+  return finish(st);
+}
+
+int visar_batch_download(visar_batch *b, const visar_image *host, size_t n) {
+  if (!b || (n > 0 && !host) || n != b->plan.inputs.size()) return report_error(VISAR_INVALID_ARGUMENT, "InvalidArgument");
+  Plan &P = b->plan;
+  cudaError_t e = cudaSetDevice(P.dev);
+  if (e != cudaSuccess) return cuda_status(e);
+  const cudaStream_t st = run_stream(P);
+  for (size_t i = 0; i < n; i++) {
+    const Buf &s = P.outs.empty() ? P.inputs[i] : P.outs.back()[i];
+    if (!host[i].data || !same_shape(host[i], s)) return report_error(VISAR_SIZE_MISMATCH, "SizeMismatch");
+    const size_t rb = (size_t)s.v.w * s.v.cn * depth_size(s.depth);
+    e = cudaMemcpy2DAsync(host[i].data, host[i].stride, s.v.p, (size_t)s.v.stride, rb, (size_t)s.v.h, cudaMemcpyDeviceToHost, st);
+    if (e != cudaSuccess) return cuda_status(e);
+  }
+  return finish(st);
+}
+
+int visar_batch_profile(visar_batch *b, int enable) {
+  if (!b) return report_error(VISAR_INVALID_ARGUMENT, "InvalidArgument");
+  Plan &P = b->plan;
+  cudaError_t e = cudaSetDevice(P.dev);
+  if (e != cudaSuccess) return cuda_status(e);
+  P.prof = enable != 0;
+  P.prof_valid = false;
+  while (P.prof && P.evs.size() < 2 * P.nlaunch) {
+    cudaEvent_t ev;
+    e = cudaEventCreate(&ev);
+    if (e != cudaSuccess) return cuda_status(e);
+    P.evs.push_back(ev);
+  }
+  return VISAR_OK;
+}
+
+int visar_batch_launch_stat_get(const visar_batch *b, size_t i, visar_batch_launch_stat *out) {
+  if (!b || !out || i >= b->plan.nlaunch) return report_error(VISAR_INVALID_ARGUMENT, "InvalidArgument");
+  const Plan &P = b->plan;
+  size_t j = 0;
+  for (const Step &s : P.steps)
+    for (const Launch &L : s.launches) {
+      if (j++ != i) continue;
+      std::memset(out, 0, sizeof(*out));
+      std::snprintf(out->name, sizeof(out->name), "%s%s", launch_key(L).c_str(), launch_suffix(L));
+      out->stage = L.stage;
+      out->images = L.imgs.size();
+      out->tiles = (size_t)L.total;
+      out->bytes = L.bytes;
+      out->grid = L.grid;
+      if (P.prof_valid) {
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, P.evs[2 * i], P.evs[2 * i + 1]) == cudaSuccess) out->ms = ms;
+        else cudaGetLastError();
+      }
+      return VISAR_OK;
+    }
+  return report_error(VISAR_INVALID_ARGUMENT, "InvalidArgument");
 }
 
 int visar_tune_load(const char *path) {
