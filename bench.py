@@ -1,21 +1,31 @@
 """Benchmark of the imgproc stencil-and-warp path on B200.
 
-Workload (default, `plain-1080p`): one 1920x1080 u8 BGR frame (gradient +
-noise + 32 rectangles, seeded) run through the plain per-call C ABI:
-resize INTER_LINEAR -> 1280x720, resize INTER_AREA -> 960x540 (exact half),
-warpAffine INTER_LINEAR BORDER_CONSTANT 0 (seeded rotation +-30 deg, scale
-0.8-1.2, translation +-50 px), warpPerspective INTER_LINEAR (corners jittered
-+-80 px), plus one 1920x1080 f32 N(0,1) frame through GaussianBlur 7x7
-sigma 1.5. One step = those five calls. Gpix/s counts input pixels
-(width x height) once per call.
+Workloads (`--workload`):
 
-  value : inputs resident in HBM, CUDA events on the launching stream,
-          L2 flushed (256 MiB write) before every timed step
-  e2e   : the same calls on pinned host buffers through the C ABI, so every
-          step includes the host->device and device->host copies
-  roofline : the dominant kernel (most total time), algorithmic bytes
-          (input + output image bytes) / its average event-timed duration,
-          against MEASURED_PEAKS.json's HBM copy bandwidth
+  batched-mixed (default): 256 uint8 images, width uniform 64-4096, height
+      uniform 64-2160, 1 or 3 channels (p = 0.5 each), content as the
+      640x480 case (gradient + noise + rectangles, seeded). Pipeline: gray
+      (3-channel images) -> GaussianBlur 5x5 -> morphologyEx OPEN 5x5
+      ELLIPSE -> resize INTER_LINEAR to half size. One step = the whole
+      batch through the batched form (persistent tile-queue launches, one
+      per stage pass and shape class, replayed as one CUDA graph). The plain
+      per-call drop-in runs the same images call by call on the same GPU
+      beside it, and the two results are compared.
+  plain-1080p: one 1920x1080 u8 BGR frame through resize linear -> 720p,
+      resize area -> 960x540, warpAffine, warpPerspective, plus one f32
+      N(0,1) frame through GaussianBlur 7x7 sigma 1.5, call by call.
+
+Gpix/s counts input pixels (width x height) once per image per step.
+
+  value : inputs resident in HBM; CUDA events on the launching stream. The
+          batched inputs (1.2 GB) are larger than L2; plain-1080p flushes L2
+          (256 MiB write) before every timed step.
+  e2e   : the same work through the public API from pinned host buffers:
+          host->device copy of every input and device->host copy of every
+          result inside each timed step.
+  roofline : the dominant kernel (most time): its algorithmic bytes (every
+          input and output byte once) / its CUDA-event duration, against
+          MEASURED_PEAKS.json's HBM copy bandwidth.
 
 `--impl reference` times VISAR's CPU path on the host cores instead: the
 C++ restatement in oracle/ (VISAR itself is Zig and has no toolchain here).
@@ -36,66 +46,10 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-W, H = 1920, 1080
-OPS = [
-    # name, input bytes, output bytes, input pixels
-    ("resize_linear_720p", W * H * 3, 1280 * 720 * 3, W * H),
-    ("resize_area_half", W * H * 3, 960 * 540 * 3, W * H),
-    ("warp_affine", W * H * 3, W * H * 3, W * H),
-    ("warp_perspective", W * H * 3, W * H * 3, W * H),
-    ("gaussian_f32_7x7", W * H * 4, W * H * 4, W * H),
-]
-PIX_PER_STEP = sum(o[3] for o in OPS)
-ALG_BYTES = {o[0]: o[1] + o[2] for o in OPS}
-H2D_BYTES = 4 * W * H * 3 + W * H * 4
-D2H_BYTES = sum(o[2] for o in OPS)
+METRIC = "Gpix/s bit-exact (served/batched vs per-call plain, 1 B200); p50/p99 latency"
 
 
-def make_inputs():
-    from visar_b200 import synth
-    img = synth.base_image(H, W, 3, nrect=32, seed=1)
-    f = synth.normal_f32(H, W, 1, seed=2)
-    maff = synth.affine_params(W, H, seed=3)
-    mper = synth.perspective_params(W, H, seed=4)
-    return img, f, maff, mper
-
-
-def run_step(m, img, f, maff, mper, outs):
-    """The five calls of one step, through module `m` (the CUDA binding or the oracle)."""
-    m.resize(img, (1280, 720), 1, dst=outs[0])
-    m.resize(img, (960, 540), 3, dst=outs[1])
-    m.warp_affine(img, maff, (W, H), 1, 0, 0.0, dst=outs[2])
-    m.warp_perspective(img, mper, (W, H), 1, 0, 0.0, dst=outs[3])
-    m.gaussian_blur(f, (7, 7), 1.5, 0, 4, dst=outs[4])
-
-
-def op_call(m, name, img, f, maff, mper, outs):
-    i = [o[0] for o in OPS].index(name)
-    if i == 0:
-        m.resize(img, (1280, 720), 1, dst=outs[0])
-    elif i == 1:
-        m.resize(img, (960, 540), 3, dst=outs[1])
-    elif i == 2:
-        m.warp_affine(img, maff, (W, H), 1, 0, 0.0, dst=outs[2])
-    elif i == 3:
-        m.warp_perspective(img, mper, (W, H), 1, 0, 0.0, dst=outs[3])
-    else:
-        m.gaussian_blur(f, (7, 7), 1.5, 0, 4, dst=outs[4])
-
-
-def alloc_outs(like_u8, like_f32, torch=None, pinned=False):
-    shapes = [((720, 1280, 3), np.uint8), ((540, 960, 3), np.uint8), ((H, W, 3), np.uint8), ((H, W, 3), np.uint8),
-              ((H, W), np.float32)]
-    outs = []
-    for shp, dt in shapes:
-        if torch is not None and not pinned:
-            outs.append(torch.empty(shp, dtype=torch.uint8 if dt == np.uint8 else torch.float32, device="cuda"))
-        elif torch is not None and pinned:
-            outs.append(torch.empty(shp, dtype=torch.uint8 if dt == np.uint8 else torch.float32, pin_memory=True).numpy())
-        else:
-            outs.append(np.empty(shp, dt))
-    return outs
-
+# ------------------------------------------------------------------ common
 
 def load_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -104,6 +58,14 @@ def load_peaks():
             d = json.load(fh)
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def load_traffic(workload, kernel):
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as fh:
+        return json.load(fh).get(workload, {}).get(kernel)
 
 
 class Clocks:
@@ -164,22 +126,6 @@ class Clocks:
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(img, f, maff, mper, budget_s=12.0, max_steps=20):
-    """The oracle (C++ restatement of VISAR's CPU path) with all host threads, on a bounded sample."""
-    from oracle import oracle as O
-    O.set_num_threads(0)
-    outs = alloc_outs(None, None)
-    run_step(O, img, f, maff, mper, outs)  # warm-up
-    t0 = time.perf_counter()
-    n = 0
-    while n < max_steps and (time.perf_counter() - t0) < budget_s:
-        run_step(O, img, f, maff, mper, outs)
-        n += 1
-    dt = time.perf_counter() - t0
-    return {"value": PIX_PER_STEP * n / dt / 1e9, "unit": "Gpix/s", "cores": O.get_num_threads(), "kind": "port",
-            "sample": f"{n} steps of the plain-1080p workload ({n * 5} calls, {PIX_PER_STEP * n / 1e6:.1f} MP) in {dt:.1f} s"}
-
-
 def dist_setup(n):
     if n <= 1 or "RANK" not in os.environ:
         return 0, 1, None
@@ -194,14 +140,413 @@ def dist_setup(n):
     return rank, world, dist
 
 
-def bench_reference(args):
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
-        return 0
+class Ctx:
+    """Per-process GPU context: a dedicated stream shared by torch, the events
+    and the library (torch's default stream has a NULL handle, which the
+    library reads as "use your own stream"), barriers and max-over-ranks."""
+
+    def __init__(self, args):
+        import torch
+        self.torch = torch
+        self.rank, self.world, self.dist = dist_setup(args.gpus)
+        if self.dist is None:
+            torch.cuda.set_device(0)
+        import visar_b200 as vb
+        self.vb = vb
+        self.dev = torch.cuda.current_device()
+        self.stream = torch.cuda.Stream()
+        torch.cuda.set_stream(self.stream)
+        vb.set_stream(self.stream)
+
+    def barrier(self):
+        self.torch.cuda.synchronize()
+        if self.dist is not None:
+            self.dist.barrier()
+
+    def max_over_ranks(self, x):
+        if self.dist is None:
+            return x
+        t = self.torch.tensor([x], dtype=self.torch.float64, device="cuda")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed(self, fn, steps, before=None):
+        """Total ms of `steps` calls of fn, CUDA events on the stream around each."""
+        torch = self.torch
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for i in range(steps):
+            if before is not None:
+                before(i)
+            ev[i][0].record(self.stream)
+            fn()
+            ev[i][1].record(self.stream)
+        torch.cuda.synchronize()
+        return sum(a.elapsed_time(b) for a, b in ev)
+
+    def close(self):
+        if self.dist is not None:
+            self.dist.barrier()
+            self.dist.destroy_process_group()
+
+
+# ----------------------------------------------------------- batched-mixed
+
+N_IMAGES = 256
+MIX_SEED = 2
+
+
+def mixed_shapes():
+    from visar_b200 import synth
+    return synth.mixed_shapes(N_IMAGES, seed=MIX_SEED)
+
+
+def c2_stages(B):
+    return [B.gray(), B.gaussian((5, 5), 0.0, 0.0, 4), B.morphology(2, 2, (5, 5), 1), B.resize(0.5, 0.5, 1)]
+
+
+def half_dims(h, w):
+    return max(1, round(h * 0.5)), max(1, round(w * 0.5))
+
+
+def c2_oracle_image(O, x):
+    """The pipeline of one image through module O (the oracle)."""
+    y = x if x.ndim == 2 else O.cvt_color(x, 6)
+    y = O.gaussian_blur(y, (5, 5), 0, 0, 4)
+    y = O.morphology(y, 2, 2, (5, 5))
+    h, w = half_dims(y.shape[0], y.shape[1])
+    return y if (h, w) == y.shape[:2] else O.resize(y, (w, h), 1)
+
+
+def c2_cpu_sample(budget_s, max_images=N_IMAGES):
+    """Times the oracle on a bounded prefix of the batch (image generation untimed);
+    returns (Gpix/s, images, MP, s, threads)."""
+    from oracle import oracle as O
+    from visar_b200 import synth
+    O.set_num_threads(0)
+    shapes = mixed_shapes()
+    c2_oracle_image(O, synth.base_image(64, 64, 3, nrect=1, seed=0))  # warm-up
+    n = px = 0
+    dt = 0.0
+    for k, (h, w, c) in enumerate(shapes[:max_images]):
+        x = synth.base_image(h, w, c, nrect=8, seed=10_000 + k)
+        t0 = time.perf_counter()
+        c2_oracle_image(O, x)
+        dt += time.perf_counter() - t0
+        n += 1
+        px += h * w
+        if dt > budget_s:
+            break
+    return px / dt / 1e9, n, px / 1e6, dt, O.get_num_threads()
+
+
+def bench_batched(args, ctx):
+    torch, vb = ctx.torch, ctx.vb
+    from visar_b200 import batch as B
+    from visar_b200 import synth
+    shapes = mixed_shapes()
+    plan = B.Batch([(h, w, c, np.uint8) for (h, w, c) in shapes], c2_stages(B))
+    for k, (h, w, c) in enumerate(shapes):
+        plan.input(k).copy_(synth.base_image_torch(h, w, c, nrect=8, seed=10_000 + k))
+    info = plan.info()
+    px_step = info["pixels_in"]
+    ins = [plan.input(k) for k in range(len(shapes))]
+    vb.set_async(True)
+
+    # ------------------------------------------------ value: graph replay
+    for _ in range(args.warmup):
+        plan.run_graph()
+    ctx.barrier()
+    with Clocks(ctx.dev) as clk:
+        ms = ctx.timed(plan.run_graph, args.steps)
+    ctx.barrier()
+    ms_step = ctx.max_over_ranks(ms) / args.steps
+    value = px_step * ctx.world / (ms_step / 1e3) / 1e9
+    clocks = clk.summary()
+
+    # --------------------------------------- plain per-call drop-in, same GPU
+    outs = []
+    for x in ins:
+        c = 1 if x.ndim == 2 else x.shape[2]
+        h, w = x.shape[:2]
+        hh, ww = half_dims(h, w)
+        outs.append((torch.empty((h, w), dtype=torch.uint8, device="cuda") if c == 3 else None,
+                     torch.empty((h, w), dtype=torch.uint8, device="cuda"),
+                     torch.empty((h, w), dtype=torch.uint8, device="cuda"),
+                     torch.empty((hh, ww), dtype=torch.uint8, device="cuda")))
+
+    def plain_step():
+        for x, (g, gb, op, rs) in zip(ins, outs):
+            y = vb.cvt_color(x, 6, dst=g) if g is not None else x
+            vb.gaussian_blur(y, (5, 5), 0, 0, 4, dst=gb)
+            vb.morphology(gb, 2, 2, (5, 5), 1, dst=op)
+            if rs.shape != op.shape:
+                vb.resize(op, (rs.shape[1], rs.shape[0]), 1, dst=rs)
+
+    plain_step()
+    ctx.barrier()
+    p_steps = max(2, min(args.steps, 5))
+    p_ms = ctx.max_over_ranks(ctx.timed(plain_step, p_steps)) / p_steps
+    plain = px_step * ctx.world / (p_ms / 1e3) / 1e9
+    for k in range(len(ins)):  # the two arms agree bit for bit
+        ref = outs[k][3] if outs[k][3].shape != outs[k][2].shape else outs[k][2]
+        if not torch.equal(ref, plan.output(k)):
+            raise AssertionError(f"batched and per-call outputs differ for image {k}")
+
+    # ------------------------------- per-launch timing for the roofline (eager)
+    plan.profile(True)
+    per = {}
+    for r in range(max(3, args.steps // 2)):
+        plan.run()
+        torch.cuda.synchronize()
+        if r == 0:
+            continue
+        for st in plan.launch_stats():
+            key = f"s{st['stage']}:{st['name']}"
+            d = per.setdefault(key, {"ms": [], "bytes": st["bytes"], "images": st["images"], "tiles": st["tiles"],
+                                     "grid": st["grid"]})
+            d["ms"].append(st["ms"])
+    plan.profile(False)
+    kernels = {k: {"ms": float(np.mean(v["ms"])), "bytes": v["bytes"], "images": v["images"], "tiles": v["tiles"],
+                   "grid": v["grid"], "gbs": v["bytes"] / (np.mean(v["ms"]) / 1e3) / 1e9} for k, v in per.items()}
+    dom = max(kernels, key=lambda k: kernels[k]["ms"])
+    peak, peak_kind = load_peaks()
+    achieved = kernels[dom]["gbs"]
+    all_ms = sum(v["ms"] for v in kernels.values())
+    pipeline_gbs = info["bytes_moved"] / (ms_step / 1e3) / 1e9
+
+    # ---------------------------------------------- e2e through the public API
+    hosts = [torch.empty(tuple(x.shape), dtype=torch.uint8, pin_memory=True).numpy() for x in ins]
+    for h, x in zip(hosts, ins):
+        h[...] = x.cpu().numpy()
+    houts = [torch.empty(tuple(plan.output(k).shape), dtype=torch.uint8, pin_memory=True).numpy()
+             for k in range(len(ins))]
+    h2d = sum(h.nbytes for h in hosts)
+    d2h = sum(h.nbytes for h in houts)
+
+    def e2e_step():
+        plan.upload(hosts)
+        plan.run_graph()
+        plan.download(houts)
+
+    e2e_step()
+    ctx.barrier()
+    e_steps = max(2, min(args.steps, 5))
+    e_ms = ctx.max_over_ranks(ctx.timed(e2e_step, e_steps)) / e_steps
+    e2e = px_step * ctx.world / (e_ms / 1e3) / 1e9
+    vb.set_async(False)
+    if not np.array_equal(houts[0], plan.output(0).cpu().numpy()):
+        raise AssertionError("downloaded output differs from the device result")
+
+    cpu = None
+    if ctx.rank == 0 and ctx.world == 1 and not args.no_cpu_baseline:
+        v, n, mp, dt, cores = c2_cpu_sample(10.0)
+        cpu = {"value": v, "unit": "Gpix/s", "cores": cores, "kind": "port",
+               "sample": f"first {n} of the {N_IMAGES} images ({mp:.1f} MP) through the 4-stage pipeline in {dt:.1f} s"}
+    return {
+        "metric": METRIC, "value": value, "unit": "Gpix/s", "n_gpus": ctx.world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": "batched-mixed", "images": N_IMAGES, "shapes": "w U[64,4096], h U[64,2160], 1|3 ch",
+                   "stages": ["gray", "gaussian 5x5", "open 5x5 ellipse", "resize linear 0.5x"],
+                   "pixels_per_step": px_step, "bytes_per_step": info["bytes_moved"],
+                   "pipeline_gbs": pipeline_gbs, "pipeline_frac": pipeline_gbs / peak,
+                   "launches_per_step": info["launches"], "fallback_calls": info["fallback_calls"],
+                   "plain_gpix_s": plain, "plain_ms_per_step": p_ms, "speedup_vs_plain": value / plain,
+                   "exec": "one CUDA graph per step (persistent tile-queue kernels)",
+                   "l2": "inputs (1.2 GB) larger than L2", "parallelism": f"replicas{ctx.world}",
+                   "kernels": kernels},
+        "e2e": {"value": e2e, "unit": "Gpix/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e_ms},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": load_traffic("batched-mixed", dom.split(":", 1)[1]),
+                     "alg_bytes_per_launch": kernels[dom]["bytes"], "share_of_kernel_time": kernels[dom]["ms"] / all_ms},
+        "cpu_baseline": cpu,
+        "clocks": clocks,
+        "gpu_launches": info["launches"] * args.steps,
+    }
+
+
+def reference_batched(args):
+    """The oracle port on the host cores: each step a fixed bounded sample of the batch."""
+    from oracle import oracle as O
+    from visar_b200 import synth
+    O.set_num_threads(0)
+    shapes = mixed_shapes()
+    sample, px = [], 0
+    for k, (h, w, c) in enumerate(shapes):  # about 25 MP per step
+        sample.append(synth.base_image(h, w, c, nrect=8, seed=10_000 + k))
+        px += h * w
+        if px >= 25e6:
+            break
+    for x in sample:
+        c2_oracle_image(O, x)
+    steps = max(1, min(args.steps, 10))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        for x in sample:
+            c2_oracle_image(O, x)
+    dt = time.perf_counter() - t0
+    v = px * steps / dt / 1e9
+    return {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "Gpix/s", "n_gpus": args.gpus, "steps": steps,
+        "warmup": args.warmup, "ms_per_step": dt / steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": "batched-mixed", "images": N_IMAGES,
+                   "impl": "VISAR CPU path (C++ restatement, oracle/), all host threads"},
+        "cpu_baseline": {"value": v, "unit": "Gpix/s", "cores": O.get_num_threads(), "kind": "port",
+                         "sample": f"first {len(sample)} images of the batch ({px / 1e6:.1f} MP) per step"},
+        "e2e": {"value": v, "unit": "Gpix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+# ------------------------------------------------------------- plain-1080p
+
+W, H = 1920, 1080
+OPS = [
+    # name, input bytes, output bytes, input pixels
+    ("resize_linear_720p", W * H * 3, 1280 * 720 * 3, W * H),
+    ("resize_area_half", W * H * 3, 960 * 540 * 3, W * H),
+    ("warp_affine", W * H * 3, W * H * 3, W * H),
+    ("warp_perspective", W * H * 3, W * H * 3, W * H),
+    ("gaussian_f32_7x7", W * H * 4, W * H * 4, W * H),
+]
+PIX_PER_STEP = sum(o[3] for o in OPS)
+ALG_BYTES = {o[0]: o[1] + o[2] for o in OPS}
+H2D_BYTES = 4 * W * H * 3 + W * H * 4
+D2H_BYTES = sum(o[2] for o in OPS)
+
+
+def make_inputs():
+    from visar_b200 import synth
+    img = synth.base_image(H, W, 3, nrect=32, seed=1)
+    f = synth.normal_f32(H, W, 1, seed=2)
+    maff = synth.affine_params(W, H, seed=3)
+    mper = synth.perspective_params(W, H, seed=4)
+    return img, f, maff, mper
+
+
+def op_call(m, name, img, f, maff, mper, outs):
+    i = [o[0] for o in OPS].index(name)
+    if i == 0:
+        m.resize(img, (1280, 720), 1, dst=outs[0])
+    elif i == 1:
+        m.resize(img, (960, 540), 3, dst=outs[1])
+    elif i == 2:
+        m.warp_affine(img, maff, (W, H), 1, 0, 0.0, dst=outs[2])
+    elif i == 3:
+        m.warp_perspective(img, mper, (W, H), 1, 0, 0.0, dst=outs[3])
+    else:
+        m.gaussian_blur(f, (7, 7), 1.5, 0, 4, dst=outs[4])
+
+
+def run_step(m, img, f, maff, mper, outs):
+    """The five calls of one step, through module `m` (the CUDA binding or the oracle)."""
+    for name, _, _, _ in OPS:
+        op_call(m, name, img, f, maff, mper, outs)
+
+
+def alloc_outs(torch=None, pinned=False):
+    shapes = [((720, 1280, 3), np.uint8), ((540, 960, 3), np.uint8), ((H, W, 3), np.uint8), ((H, W, 3), np.uint8),
+              ((H, W), np.float32)]
+    outs = []
+    for shp, dt in shapes:
+        if torch is not None and not pinned:
+            outs.append(torch.empty(shp, dtype=torch.uint8 if dt == np.uint8 else torch.float32, device="cuda"))
+        elif torch is not None and pinned:
+            outs.append(torch.empty(shp, dtype=torch.uint8 if dt == np.uint8 else torch.float32, pin_memory=True).numpy())
+        else:
+            outs.append(np.empty(shp, dt))
+    return outs
+
+
+def plain_cpu_baseline(img, f, maff, mper, budget_s=12.0, max_steps=20):
+    """The oracle with all host threads, on a bounded sample."""
+    from oracle import oracle as O
+    O.set_num_threads(0)
+    outs = alloc_outs()
+    run_step(O, img, f, maff, mper, outs)  # warm-up
+    t0 = time.perf_counter()
+    n = 0
+    while n < max_steps and (time.perf_counter() - t0) < budget_s:
+        run_step(O, img, f, maff, mper, outs)
+        n += 1
+    dt = time.perf_counter() - t0
+    return {"value": PIX_PER_STEP * n / dt / 1e9, "unit": "Gpix/s", "cores": O.get_num_threads(), "kind": "port",
+            "sample": f"{n} steps of the plain-1080p workload ({n * 5} calls, {PIX_PER_STEP * n / 1e6:.1f} MP) in {dt:.1f} s"}
+
+
+def bench_plain(args, ctx):
+    torch, vb = ctx.torch, ctx.vb
+    img, f, maff, mper = make_inputs()
+    d_img = torch.from_numpy(img).cuda()
+    d_f = torch.from_numpy(f).cuda()
+    d_outs = alloc_outs(torch)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    vb.set_async(True)
+    for _ in range(args.warmup):
+        run_step(vb, d_img, d_f, maff, mper, d_outs)
+    ctx.barrier()
+    n0 = vb.launch_count()
+    with Clocks(ctx.dev) as clk:
+        ms = ctx.timed(lambda: run_step(vb, d_img, d_f, maff, mper, d_outs), args.steps,
+                       before=lambda i: flush.fill_(i & 0xFF))
+    launches = vb.launch_count() - n0
+    ctx.barrier()
+    ms_step = ctx.max_over_ranks(ms) / args.steps
+    value = PIX_PER_STEP * ctx.world / (ms_step / 1e3) / 1e9
+    clocks = clk.summary()
+
+    per_op = {}
+    for name, _, _, _ in OPS:
+        for _ in range(3):
+            op_call(vb, name, d_img, d_f, maff, mper, d_outs)
+        n = max(5, args.steps // 2)
+        per_op[name] = ctx.timed(lambda: op_call(vb, name, d_img, d_f, maff, mper, d_outs), n,
+                                 before=lambda i: flush.fill_(i & 0xFF)) / n
+    vb.set_async(False)
+    dom = max(per_op, key=lambda k: per_op[k])
+    peak, peak_kind = load_peaks()
+    achieved = ALG_BYTES[dom] / (per_op[dom] / 1e3) / 1e9
+
+    h_img = torch.empty(img.shape, dtype=torch.uint8, pin_memory=True).numpy()
+    h_img[...] = img
+    h_f = torch.empty(f.shape, dtype=torch.float32, pin_memory=True).numpy()
+    h_f[...] = f
+    h_outs = alloc_outs(torch, pinned=True)
+    for _ in range(args.warmup):
+        run_step(vb, h_img, h_f, maff, mper, h_outs)
+    ctx.barrier()
+    e_ms = ctx.max_over_ranks(ctx.timed(lambda: run_step(vb, h_img, h_f, maff, mper, h_outs), args.steps,
+                                        before=lambda i: flush.fill_(i & 0xFF))) / args.steps
+    e2e = PIX_PER_STEP * ctx.world / (e_ms / 1e3) / 1e9
+    ctx.barrier()
+    cpu = None
+    if ctx.rank == 0 and ctx.world == 1 and not args.no_cpu_baseline:
+        cpu = plain_cpu_baseline(img, f, maff, mper)
+    return {
+        "metric": METRIC, "value": value, "unit": "Gpix/s", "n_gpus": ctx.world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8+f32", "data": "synthetic",
+        "config": {"workload": "plain-1080p", "frame": f"{W}x{H}x3 u8 + {W}x{H}x1 f32",
+                   "ops": [o[0] for o in OPS], "pixels_per_step": PIX_PER_STEP,
+                   "l2": "flushed before every timed step (256 MiB write)", "parallelism": f"replicas{ctx.world}",
+                   "per_op_ms": per_op},
+        "e2e": {"value": e2e, "unit": "Gpix/s", "h2d_bytes_per_step": H2D_BYTES, "d2h_bytes_per_step": D2H_BYTES,
+                "ms_per_step": e_ms},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": load_traffic("plain-1080p", dom),
+                     "alg_bytes_per_launch": ALG_BYTES[dom]},
+        "cpu_baseline": cpu,
+        "clocks": clocks,
+        "gpu_launches": launches,
+    }
+
+
+def reference_plain(args):
     from oracle import oracle as O
     O.set_num_threads(0)
     img, f, maff, mper = make_inputs()
-    outs = alloc_outs(None, None)
+    outs = alloc_outs()
     for _ in range(max(1, min(args.warmup, 2))):
         run_step(O, img, f, maff, mper, outs)
     steps = max(1, min(args.steps, 10))
@@ -210,8 +555,8 @@ def bench_reference(args):
         run_step(O, img, f, maff, mper, outs)
     dt = time.perf_counter() - t0
     v = PIX_PER_STEP * steps / dt / 1e9
-    line = {
-        "impl": "reference", "metric": "Gpix/s (plain per-call, bit-exact)", "value": v, "unit": "Gpix/s",
+    return {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "Gpix/s",
         "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup, "ms_per_step": dt / steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8+f32", "data": "synthetic",
         "config": {"workload": "plain-1080p", "frame": f"{W}x{H}x3 u8 + {W}x{H}x1 f32",
@@ -220,8 +565,11 @@ def bench_reference(args):
                          "sample": f"{steps} steps of plain-1080p"},
         "e2e": {"value": v, "unit": "Gpix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
-    print(json.dumps(line), flush=True)
-    return 0
+
+
+# -------------------------------------------------------------------- main
+
+WORKLOADS = {"batched-mixed": (bench_batched, reference_batched), "plain-1080p": (bench_plain, reference_plain)}
 
 
 def main():
@@ -230,133 +578,22 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="batched-mixed", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
+    ours, ref = WORKLOADS[args.workload]
     if args.impl == "reference":
-        return bench_reference(args)
+        if int(os.environ.get("RANK", "0")) != 0:
+            return 0
+        print(json.dumps(ref(args)), flush=True)
+        return 0
     args.warmup = max(3, args.warmup)
-
-    import torch
-    rank, world, dist = dist_setup(args.gpus)
-    if dist is None:
-        torch.cuda.set_device(0)
-    import visar_b200 as vb
-    dev = torch.cuda.current_device()
-    # A real stream (torch's default stream has a NULL handle, which the
-    # library reads as "use your own stream"): events, the L2 flush and the
-    # library's kernels are all ordered on it.
-    stream = torch.cuda.Stream()
-    torch.cuda.set_stream(stream)
-    vb.set_stream(stream)
-
-    img, f, maff, mper = make_inputs()
-    d_img = torch.from_numpy(img).cuda()
-    d_f = torch.from_numpy(f).cuda()
-    d_outs = alloc_outs(None, None, torch=torch)
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-
-    def barrier():
-        torch.cuda.synchronize()
-        if dist is not None:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    # ---------------------------------------------------------- value (HBM-resident)
-    vb.set_async(True)
-    for _ in range(args.warmup):
-        run_step(vb, d_img, d_f, maff, mper, d_outs)
-    barrier()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    n0 = vb.launch_count()
-    with Clocks(dev) as clk:
-        for i in range(args.steps):
-            flush.fill_(i & 0xFF)
-            ev[i][0].record(stream)
-            run_step(vb, d_img, d_f, maff, mper, d_outs)
-            ev[i][1].record(stream)
-        torch.cuda.synchronize()
-    launches = vb.launch_count() - n0
-    barrier()
-    ms_total = sum(a.elapsed_time(b) for a, b in ev)
-    ms_total = max_over_ranks(ms_total)
-    ms_step = ms_total / args.steps
-    value = PIX_PER_STEP * world / (ms_step / 1e3) / 1e9
-    clocks = clk.summary()
-
-    # ------------------------------------------------- per-kernel roofline (device)
-    per_op = {}
-    for name, _, _, _ in OPS:
-        for _ in range(3):
-            op_call(vb, name, d_img, d_f, maff, mper, d_outs)
-        es = []
-        for i in range(max(5, args.steps // 2)):
-            flush.fill_(i & 0xFF)
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-            op_call(vb, name, d_img, d_f, maff, mper, d_outs)
-            b.record(stream)
-            es.append((a, b))
-        torch.cuda.synchronize()
-        per_op[name] = float(np.mean([a.elapsed_time(b) for a, b in es]))
-    vb.set_async(False)
-    dom = max(per_op, key=lambda k: per_op[k])
-    peak, peak_kind = load_peaks()
-    achieved = ALG_BYTES[dom] / (per_op[dom] / 1e3) / 1e9
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tpath):
-        with open(tpath) as fh:
-            traffic = json.load(fh).get("plain-1080p", {}).get(dom)
-
-    # ------------------------------------------------------- e2e (pinned host buffers)
-    h_img = torch.empty(img.shape, dtype=torch.uint8, pin_memory=True).numpy()
-    h_img[...] = img
-    h_f = torch.empty(f.shape, dtype=torch.float32, pin_memory=True).numpy()
-    h_f[...] = f
-    h_outs = alloc_outs(None, None, torch=torch, pinned=True)
-    for _ in range(args.warmup):
-        run_step(vb, h_img, h_f, maff, mper, h_outs)
-    barrier()
-    e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    for i in range(args.steps):
-        flush.fill_(i & 0xFF)
-        e_ev[i][0].record(stream)
-        run_step(vb, h_img, h_f, maff, mper, h_outs)
-        e_ev[i][1].record(stream)
-    torch.cuda.synchronize()
-    e_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in e_ev)) / args.steps
-    e2e = PIX_PER_STEP * world / (e_ms / 1e3) / 1e9
-    barrier()
-
-    if rank == 0:
-        cpu = None if args.no_cpu_baseline or world > 1 else cpu_baseline(img, f, maff, mper)
-        line = {
-            "metric": "Gpix/s (plain per-call, bit-exact)", "value": value, "unit": "Gpix/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "u8+f32", "data": "synthetic",
-            "config": {"workload": "plain-1080p", "frame": f"{W}x{H}x3 u8 + {W}x{H}x1 f32",
-                       "ops": [o[0] for o in OPS], "pixels_per_step": PIX_PER_STEP,
-                       "l2": "flushed before every timed step (256 MiB write)", "parallelism": f"replicas{world}",
-                       "per_op_ms": per_op},
-            "e2e": {"value": e2e, "unit": "Gpix/s", "h2d_bytes_per_step": H2D_BYTES, "d2h_bytes_per_step": D2H_BYTES,
-                    "ms_per_step": e_ms},
-            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
-                         "alg_bytes_per_launch": ALG_BYTES[dom]},
-            "cpu_baseline": cpu,
-            "clocks": clocks,
-            "gpu_launches": launches,
-        }
+    ctx = Ctx(args)
+    line = ours(args, ctx)
+    ctx.barrier()
+    if ctx.rank == 0:
         print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    ctx.close()
     return 0
 
 
