@@ -71,7 +71,7 @@ struct Buf {
   int input = -1;  // index of the plan input this buffer is, else -1
 };
 
-enum OpKind { kOpGauss, kOpMorph, kOpGray, kOpHalf, kOpLinear, kOpLut, kOpWarpAff, kOpWarpPer };
+enum OpKind { kOpGauss, kOpMorph, kOpGray, kOpHalf, kOpLinear, kOpLut, kOpWarpAff, kOpWarpPer, kOpGaussStrip, kOpMorphStrip };
 
 const char *op_name(int op) {
   switch (op) {
@@ -83,6 +83,8 @@ const char *op_name(int op) {
     case kOpLut: return "lut";
     case kOpWarpAff: return "warp_affine";
     case kOpWarpPer: return "warp_perspective";
+    case kOpGaussStrip: return "gauss_strip";
+    case kOpMorphStrip: return "morph_strip";
   }
   return "?";
 }
@@ -98,6 +100,9 @@ struct Launch {
   int per_sm = 0;   // CTAs per SM (0: as many as fit)
   fast::FastArgs fa{};
   fast::MFArgs ma{};
+  bool fused = false;
+  int sub = 0;      // strip::ProfileId of a morphology strip launch
+  int border = 0;
   WarpArgs wa{};
   const uint8_t *lut = nullptr;
   std::vector<BImg> imgs;
@@ -225,21 +230,70 @@ std::string launch_key(const Launch &L) {
 }
 
 const char *launch_suffix(const Launch &L) {
-  if (L.op != kOpMorph) return "";
+  if (L.op != kOpMorph && L.op != kOpMorphStrip) return "";
+  if (L.fused) return L.is_max ? ".close" : ".open";
   return L.is_max ? ".max" : ".min";
 }
 
-Launch *class_of(std::vector<Launch> &ls, int op, int depth, int cn, int k, bool is_max) {
+Launch *class_of(std::vector<Launch> &ls, int op, int depth, int cn, int k, bool is_max, bool fused = false,
+                 int sub = 0) {
   for (Launch &l : ls)
-    if (l.op == op && l.depth == depth && l.cn == cn && l.k == k && l.is_max == is_max) return &l;
+    if (l.op == op && l.depth == depth && l.cn == cn && l.k == k && l.is_max == is_max && l.fused == fused &&
+        l.sub == sub)
+      return &l;
   ls.emplace_back();
   Launch &l = ls.back();
+  l.sub = sub;
   l.op = op;
   l.depth = depth;
   l.cn = cn;
   l.k = k;
   l.is_max = is_max;
+  l.fused = fused;
   return &l;
+}
+
+// The packed strip Gaussian applies when the fixed taps are g * binomial(k)
+// with g = 256 / 2^(k-1) (the sigma <= 0 tables of 3x3 and 5x5).
+bool binomial_taps(const std::vector<int64_t> &t) {
+  const int k = (int)t.size();
+  if (k != 3 && k != 5) return false;
+  static const int b3[3] = {1, 2, 1}, b5[5] = {1, 4, 6, 4, 1};
+  const int *b = k == 3 ? b3 : b5;
+  const int64_t g = k == 3 ? 64 : 16;
+  for (int j = 0; j < k; j++)
+    if (t[j] != g * b[j]) return false;
+  return true;
+}
+
+// Per-row half-widths of an element made of runs centred on the anchor
+// column (-1: empty row); false for any other element.
+bool row_profile(const std::vector<uint8_t> &mask, int kw, int kh, int *d) {
+  if (kw % 2 == 0 || kh % 2 == 0 || kh > 16) return false;
+  const int ax = kw / 2;
+  for (int y = 0; y < kh; y++) {
+    int j1 = -1, j2 = -1;
+    for (int x = 0; x < kw; x++)
+      if (mask[(size_t)y * kw + x]) {
+        if (j1 < 0) j1 = x;
+        j2 = x;
+      }
+    if (j1 < 0) {
+      d[y] = -1;
+      continue;
+    }
+    for (int x = j1; x <= j2; x++)
+      if (!mask[(size_t)y * kw + x]) return false;
+    if (ax - j1 != j2 - ax) return false;
+    d[y] = ax - j1;
+  }
+  return true;
+}
+
+// Strip halo words of a morphology launch (strip.cuh MorphStrip::HALO).
+int strip_halo(int prof, int cn, bool fused) {
+  const int m = strip::profile_maxd(prof) * (fused ? 2 : 1) * cn;
+  return std::max(1, (m + 3) / 4);
 }
 
 int gauss_tiles_x(int w, int cn, int k) {
@@ -274,6 +328,16 @@ void set_tiles(const Launch &L, BImg &b) {
       b.tiles_x = (int)ceil_div((long long)b.s.w * b.s.cn, 256 * 16);
       b.tiles_y = (int)ceil_div(b.s.h, L.rows);
       break;
+    case kOpGaussStrip: {
+      const int nw = ((L.k / 2) * L.cn + 3) / 4;
+      b.tiles_x = (int)ceil_div(((long long)b.s.w * L.cn + 3) / 4, 32 - 2 * nw);
+      b.tiles_y = (int)ceil_div(b.s.h, L.rows);
+      break;
+    }
+    case kOpMorphStrip:
+      b.tiles_x = (int)ceil_div(((long long)b.s.w * L.cn + 3) / 4, 32 - 2 * strip_halo(L.sub, L.cn, L.fused));
+      b.tiles_y = (int)ceil_div(b.s.h, L.rows);
+      break;
     default:
       b.tiles_x = (int)ceil_div(b.d.w, 32);
       b.tiles_y = (int)ceil_div(b.d.h, 32);
@@ -298,6 +362,12 @@ void tune_and_tile(Launch &L) {
       L.rows = std::min(std::max(r, 1), 64);
       break;
     }
+    case kOpGaussStrip: {
+      const int r = get("rows", 32);
+      L.rows = r == 64 ? 64 : 32;
+      break;
+    }
+    case kOpMorphStrip: L.rows = 32; break;
     default: L.rows = 8;
   }
   L.per_sm = std::max(0, get("per_sm", 0));
@@ -404,6 +474,17 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
           fallback(i, next[i], nullptr);
           continue;
         }
+        if (u8) {
+          std::vector<int64_t> t(kw);
+          gaussian_kernel_fixed(t.data(), kw, sx, 8);
+          if (binomial_taps(t)) {
+            Launch *l = class_of(ls, kOpGaussStrip, k8U, im.v.cn, kw, false);
+            l->border = border;
+            add_img(l, bimg(im.v, next[i].v), im.input);
+            u8_bytes(*l, im.v, next[i].v, 1);
+            continue;
+          }
+        }
         Launch *l = class_of(ls, kOpGauss, im.depth, im.v.cn, kw, false);
         l->fa = a;
         add_img(l, bimg(im.v, next[i].v), im.input);
@@ -426,15 +507,33 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
       else if (op == 2) { add(false); add(true); }
       else if (op == 3) { add(true); add(false); }
       const bool kernel_ok = op <= 3 && !passes.empty();
+      // OPEN / CLOSE of one iteration whose two horizontal reaches fit one
+      // halo word run as one fused strip launch; other covered shapes run
+      // pass by pass (ping-ponging through temporaries).
+      // Elements with a compiled profile run on warp strips: OPEN / CLOSE of
+      // one iteration as one fused launch, other cases pass by pass
+      // (ping-ponging through temporaries); other centred-run elements with
+      // a short reach use the band kernel pass by pass.
+      int dprof[16];
+      const int prof = row_profile(mask, kw, kh, dprof) ? strip::profile_of(dprof, kh) : strip::kProfileCount;
       std::vector<std::vector<Buf>> tmp(n);
-      std::vector<bool> fast_img(n, false);
+      std::vector<int> mode(n, 0);  // 0 fallback, 1 strip passes, 2 fused strip, 3 band passes
       for (size_t i = 0; i < n; i++) {
         const Buf &im = cur[i];
         if (!B.image(im.v.w, im.v.h, im.v.cn, im.depth, next[i])) return VISAR_OUT_OF_MEMORY;
+        const bool u8ok = kernel_ok && im.depth == k8U && (im.v.cn == 1 || im.v.cn == 3 || im.v.cn == 4) &&
+                          u8_aligned4(im.v);
         fast::MFArgs ma;
-        fast_img[i] = kernel_ok && im.depth == k8U && fast::morph_fast_args(mask, kw, kh, im.v.cn, im.v.w, ma) &&
-                      u8_aligned4(im.v);
-        if (!fast_img[i]) {
+        if (u8ok && prof < strip::kProfileCount && strip_halo(prof, im.v.cn, true) <= 8 && (op == 2 || op == 3) && it == 1) {
+          mode[i] = 2;
+          Launch *l = class_of(ls, kOpMorphStrip, k8U, im.v.cn, kh, op == 3, true, prof);
+          add_img(l, bimg(im.v, next[i].v), im.input);
+          u8_bytes(*l, im.v, next[i].v, 1);
+          continue;
+        }
+        if (u8ok && prof < strip::kProfileCount) mode[i] = 1;
+        else if (u8ok && fast::morph_fast_args(mask, kw, kh, im.v.cn, im.v.w, ma)) mode[i] = 3;
+        if (mode[i] == 0) {
           fallback(i, next[i], nullptr);
           continue;
         }
@@ -443,16 +542,26 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
         for (size_t k = 0; k < ntmp; k++)
           if (!B.image(im.v.w, im.v.h, im.v.cn, im.depth, tmp[i][k])) return VISAR_OUT_OF_MEMORY;
       }
+      for (Launch &l : ls) {
+        tune_and_tile(l);
+        step.launches.push_back(std::move(l));
+      }
+      ls.clear();
       const size_t np = passes.size();
       for (size_t p = 0; p < np && kernel_ok; p++) {
         std::vector<Launch> pl;
         for (size_t i = 0; i < n; i++) {
-          if (!fast_img[i]) continue;
+          if (mode[i] != 1 && mode[i] != 3) continue;
           const Buf &im = cur[i];
           const DImg src = p == 0 ? im.v : tmp[i][(p - 1) % 2].v;
           const DImg dst = p + 1 == np ? next[i].v : tmp[i][p % 2].v;
-          Launch *l = class_of(pl, kOpMorph, k8U, im.v.cn, kh, passes[p]);
-          fast::morph_fast_args(mask, kw, kh, im.v.cn, im.v.w, l->ma);
+          Launch *l;
+          if (mode[i] == 1) {
+            l = class_of(pl, kOpMorphStrip, k8U, im.v.cn, kh, passes[p], false, prof);
+          } else {
+            l = class_of(pl, kOpMorph, k8U, im.v.cn, kh, passes[p]);
+            fast::morph_fast_args(mask, kw, kh, im.v.cn, im.v.w, l->ma);
+          }
           add_img(l, bimg(src, dst), p == 0 ? im.input : -1);
           u8_bytes(*l, src, dst, 1);
         }
@@ -608,34 +717,14 @@ int build_all(Builder &B, const std::vector<visar_stage> &stages) {
 
 // ------------------------------------------------------------------ run
 
-std::mutex g_kattr_mu;
-std::map<const void *, int> g_occ;
+LaunchRun run_of(const Plan &P, const Launch &L) {
+  return LaunchRun{TileQ{L.d_imgs, L.d_start, (int)L.imgs.size(), L.total, P.counters + L.counter}, L.per_sm, P.num_sms,
+                   &L.grid};
+}
 
 template <class Op>
 cudaError_t run_op(const Plan &P, const Launch &L, const typename Op::Args &a, cudaStream_t st) {
-  const TileQ q{L.d_imgs, L.d_start, (int)L.imgs.size(), L.total, P.counters + L.counter};
-  const size_t smem = Op::smem(a);
-  auto kern = k_batch<Op>;
-  int occ = 0;
-  {
-    std::lock_guard<std::mutex> lk(g_kattr_mu);
-    const auto it = g_occ.find((const void *)kern);
-    if (it == g_occ.end()) {
-      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e != cudaSuccess) return e;
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, Op::kThreads, smem);
-      if (e != cudaSuccess) return e;
-      g_occ[(const void *)kern] = occ;
-    } else {
-      occ = it->second;
-    }
-  }
-  const int per_sm = L.per_sm > 0 ? std::min(L.per_sm, std::max(occ, 1)) : std::max(occ, 1);
-  const int grid = std::max(1, std::min(L.total, P.num_sms * per_sm));
-  L.grid = grid;
-  kern<<<grid, Op::kThreads, smem, st>>>(q, a);
-  note_launch();
-  return cudaGetLastError();
+  return launch_op<Op>(run_of(P, L), a, st);
 }
 
 template <class S, int K, int CN>
@@ -698,6 +787,8 @@ cudaError_t run_launch(const Plan &P, const Launch &L, cudaStream_t st) {
   if (L.total == 0) return cudaSuccess;
   const RowArgs ra{L.rows};
   switch (L.op) {
+    case kOpGaussStrip: return launch_gauss_strip(run_of(P, L), L.k, L.cn, L.rows, L.border, st);
+    case kOpMorphStrip: return launch_morph_strip(run_of(P, L), L.sub, L.cn, L.rows, L.is_max, L.fused, st);
     case kOpGauss: return L.depth == k8U ? run_gauss<uint8_t>(P, L, st) : run_gauss<float>(P, L, st);
     case kOpMorph:
       if (L.cn == 1) return run_morph<1>(P, L, st);

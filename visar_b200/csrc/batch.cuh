@@ -9,8 +9,12 @@
 // tile while the current one is processed, so the atomic's latency overlaps
 // the work.
 #pragma once
+#include <algorithm>
+#include <type_traits>
+
 #include "morphfast.cuh"
 #include "sepfast.cuh"
+#include "strip.cuh"
 #include "vb.h"
 #include "warp.cuh"
 
@@ -78,6 +82,37 @@ __global__ void __launch_bounds__(Op::kThreads) k_batch(TileQ q, typename Op::Ar
     cur = s_tile[buf];
   }
 }
+
+// Warp-granular queue: every warp claims its own tiles (lane 0 takes the
+// ticket, the warp broadcasts it); no block barrier after the prefix cache.
+template <class Op>
+__global__ void __launch_bounds__(Op::kThreads) k_batch_warp(TileQ q, typename Op::Args a) {
+  __shared__ int s_start[kStartCap + 1];
+  const bool cached = q.n <= kStartCap;
+  if (cached)
+    for (int i = threadIdx.x; i <= q.n; i += Op::kThreads) s_start[i] = q.start[i];
+  __syncthreads();
+  const int *start = cached ? s_start : q.start;
+  const int lane = threadIdx.x & 31;
+  int t = 0;
+  if (lane == 0) t = atomicAdd(q.counter, 1);
+  int cur = __shfl_sync(0xFFFFFFFFu, t, 0);
+  while (cur < q.total) {
+    if (lane == 0) t = atomicAdd(q.counter, 1);
+    const int img = find_image(start, q.n, cur);
+    const BImg &im = q.imgs[img];
+    const int local = cur - start[img];
+    const int txn = im.tiles_x;
+    Op::tile(im, a, local % txn, local / txn, lane);
+    cur = __shfl_sync(0xFFFFFFFFu, t, 0);
+  }
+}
+
+// Operations with kWarpTiles = true run under k_batch_warp (a tile per warp).
+template <class Op, class = void>
+struct WarpTiles : std::false_type {};
+template <class Op>
+struct WarpTiles<Op, std::void_t<decltype(Op::kWarpTiles)>> : std::bool_constant<Op::kWarpTiles> {};
 
 // ------------------------------------------------------------ operations
 // Each operation: kThreads, Args, host smem(Args) / tiles(w, h, Args), and
@@ -296,6 +331,35 @@ struct OpLut {
   }
 };
 
+// u8 Gaussian with binomial taps on warp strips (strip.cuh).
+template <int K, int CN, int RH>
+struct OpGaussStrip {
+  static constexpr int kThreads = 256;
+  static constexpr bool kWarpTiles = true;
+  using Args = strip::GaussArgs;
+  static size_t smem(const Args &) { return 0; }
+  static __device__ __forceinline__ void tile(const BImg &im, const Args &a, int tx, int ty, int lane) {
+    strip::gauss_strip<K, CN, RH>(im.s, im.d, a.border, tx, ty, lane);
+  }
+};
+
+struct NoArgs {
+  int unused;
+};
+
+// Erode / dilate (one pass, or two fused) with a compiled element profile
+// on warp strips (strip.cuh).
+template <class P1, class P2, int CN, int RH, bool MAX1, bool FUSED>
+struct OpMorphStrip {
+  static constexpr int kThreads = 256;
+  static constexpr bool kWarpTiles = true;
+  using Args = NoArgs;
+  static size_t smem(const Args &) { return 0; }
+  static __device__ __forceinline__ void tile(const BImg &im, const Args &, int tx, int ty, int lane) {
+    strip::MorphStrip<P1, P2, CN, RH, MAX1, FUSED>::run(im.s, im.d, tx, ty, lane);
+  }
+};
+
 struct WarpArgs {
   int interp, border;
 };
@@ -339,6 +403,84 @@ struct OpWarp {
     }
   }
 };
+
+// ----------------------------------------------------------- launching
+
+template <class Op>
+auto kernel_of() {
+  if constexpr (WarpTiles<Op>::value) return k_batch_warp<Op>;
+  else return k_batch<Op>;
+}
+
+// What one persistent launch needs: the queue, CTAs per SM (0: as many as
+// fit) and the SM count; the grid launched is reported in *grid.
+struct LaunchRun {
+  TileQ q;
+  int per_sm;
+  int num_sms;
+  int *grid;
+};
+
+// Launches Op's persistent kernel: the grid is the SMs times the CTAs per SM
+// that fit (or the tuned count), capped by the tiles (per warp for
+// warp-tile operations).
+template <class Op>
+cudaError_t launch_op(const LaunchRun &r, const typename Op::Args &a, cudaStream_t st) {
+  const size_t smem = Op::smem(a);
+  constexpr bool kWarp = WarpTiles<Op>::value;
+  auto kern = kernel_of<Op>();
+  static int occ = -1;  // per instantiation; same device type everywhere
+  if (occ < 0) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int o = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, Op::kThreads, smem);
+    if (e != cudaSuccess) return e;
+    occ = o;
+  }
+  const int per_sm = r.per_sm > 0 ? std::min(r.per_sm, std::max(occ, 1)) : std::max(occ, 1);
+  const int units = kWarp ? (int)ceil_div(r.q.total, Op::kThreads / 32) : r.q.total;
+  const int grid = std::max(1, std::min(units, r.num_sms * per_sm));
+  if (r.grid) *r.grid = grid;
+  kern<<<grid, Op::kThreads, smem, st>>>(r.q, a);
+  note_launch();
+  return cudaGetLastError();
+}
+
+// Strip launches (batch_strip*.cu). prof: strip::ProfileId of the element.
+cudaError_t launch_gauss_strip(const LaunchRun &r, int k, int cn, int rows, int border, cudaStream_t st);
+cudaError_t launch_morph_strip(const LaunchRun &r, int prof, int cn, int rows, bool max1, bool fused, cudaStream_t st);
+
+// The morphology strip launches of one channel count (one translation unit
+// each, to spread the compile).
+template <int CN>
+cudaError_t launch_morph_strip_cn(const LaunchRun &r, int prof, bool max1, bool fused, cudaStream_t st);
+
+template <class PR, int CN>
+cudaError_t launch_morph_strip_prof(const LaunchRun &r, bool max1, bool fused, cudaStream_t st) {
+  constexpr int RH = 32;
+  const NoArgs a{0};
+  if (fused)
+    return max1 ? launch_op<OpMorphStrip<PR, PR, CN, RH, true, true>>(r, a, st)
+                : launch_op<OpMorphStrip<PR, PR, CN, RH, false, true>>(r, a, st);
+  return max1 ? launch_op<OpMorphStrip<PR, PR, CN, RH, true, false>>(r, a, st)
+              : launch_op<OpMorphStrip<PR, PR, CN, RH, false, false>>(r, a, st);
+}
+
+template <int CN>
+cudaError_t launch_morph_strip_cn(const LaunchRun &r, int prof, bool max1, bool fused, cudaStream_t st) {
+  using namespace strip;
+  switch (prof) {
+    case kRect3: return launch_morph_strip_prof<ProfRect3, CN>(r, max1, fused, st);
+    case kRect5: return launch_morph_strip_prof<ProfRect5, CN>(r, max1, fused, st);
+    case kRect7: return launch_morph_strip_prof<ProfRect7, CN>(r, max1, fused, st);
+    case kCross3: return launch_morph_strip_prof<ProfCross3, CN>(r, max1, fused, st);
+    case kCross5: return launch_morph_strip_prof<ProfCross5, CN>(r, max1, fused, st);
+    case kEll5: return launch_morph_strip_prof<ProfEll5, CN>(r, max1, fused, st);
+    case kEll7: return launch_morph_strip_prof<ProfEll7, CN>(r, max1, fused, st);
+  }
+  return cudaErrorNotSupported;
+}
 
 }  // namespace bt
 }  // namespace vb

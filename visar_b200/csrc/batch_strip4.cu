@@ -1,0 +1,10 @@
+// Morphology strip launches of the batched form for 4-channel images.
+#include "batch.cuh"
+
+namespace vb {
+namespace bt {
+
+template cudaError_t launch_morph_strip_cn<4>(const LaunchRun &, int, bool, bool, cudaStream_t);
+
+}  // namespace bt
+}  // namespace vb
