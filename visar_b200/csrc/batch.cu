@@ -293,7 +293,7 @@ bool row_profile(const std::vector<uint8_t> &mask, int kw, int kh, int *d) {
 // Strip halo words of a morphology launch (strip.cuh MorphStrip::HALO).
 int strip_halo(int prof, int cn, bool fused) {
   const int m = strip::profile_maxd(prof) * (fused ? 2 : 1) * cn;
-  return std::max(1, (m + 3) / 4);
+  return std::max(1, (m + strip::kSPL - 1) / strip::kSPL);
 }
 
 int gauss_tiles_x(int w, int cn, int k) {
@@ -329,13 +329,13 @@ void set_tiles(const Launch &L, BImg &b) {
       b.tiles_y = (int)ceil_div(b.s.h, L.rows);
       break;
     case kOpGaussStrip: {
-      const int nw = ((L.k / 2) * L.cn + 3) / 4;
-      b.tiles_x = (int)ceil_div(((long long)b.s.w * L.cn + 3) / 4, 32 - 2 * nw);
+      const int halo = ((L.k / 2) * L.cn + strip::kSPL - 1) / strip::kSPL;
+      b.tiles_x = (int)ceil_div((long long)b.s.w * L.cn, strip::kSPL * (32 - 2 * halo));
       b.tiles_y = (int)ceil_div(b.s.h, L.rows);
       break;
     }
     case kOpMorphStrip:
-      b.tiles_x = (int)ceil_div(((long long)b.s.w * L.cn + 3) / 4, 32 - 2 * strip_halo(L.sub, L.cn, L.fused));
+      b.tiles_x = (int)ceil_div((long long)b.s.w * L.cn, strip::kSPL * (32 - 2 * strip_halo(L.sub, L.cn, L.fused)));
       b.tiles_y = (int)ceil_div(b.s.h, L.rows);
       break;
     default:
@@ -375,6 +375,7 @@ void tune_and_tile(Launch &L) {
 }
 
 bool u8_aligned4(const DImg &v) { return ((uintptr_t)v.p % 4 == 0) && (v.stride % 4 == 0); }
+bool u8_aligned8(const DImg &v) { return ((uintptr_t)v.p % 8 == 0) && (v.stride % 8 == 0); }
 bool aligned16(const DImg &v) { return ((uintptr_t)v.p % 16 == 0) && (v.stride % 16 == 0); }
 
 BImg bimg(const DImg &s, const DImg &d) {
@@ -477,7 +478,7 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
         if (u8) {
           std::vector<int64_t> t(kw);
           gaussian_kernel_fixed(t.data(), kw, sx, 8);
-          if (binomial_taps(t)) {
+          if (binomial_taps(t) && u8_aligned8(im.v)) {
             Launch *l = class_of(ls, kOpGaussStrip, k8U, im.v.cn, kw, false);
             l->border = border;
             add_img(l, bimg(im.v, next[i].v), im.input);
@@ -524,14 +525,15 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
         const bool u8ok = kernel_ok && im.depth == k8U && (im.v.cn == 1 || im.v.cn == 3 || im.v.cn == 4) &&
                           u8_aligned4(im.v);
         fast::MFArgs ma;
-        if (u8ok && prof < strip::kProfileCount && strip_halo(prof, im.v.cn, true) <= 8 && (op == 2 || op == 3) && it == 1) {
+        const bool strip_ok = u8ok && prof < strip::kProfileCount && u8_aligned8(im.v);
+        if (strip_ok && strip_halo(prof, im.v.cn, true) <= 8 && (op == 2 || op == 3) && it == 1) {
           mode[i] = 2;
           Launch *l = class_of(ls, kOpMorphStrip, k8U, im.v.cn, kh, op == 3, true, prof);
           add_img(l, bimg(im.v, next[i].v), im.input);
           u8_bytes(*l, im.v, next[i].v, 1);
           continue;
         }
-        if (u8ok && prof < strip::kProfileCount) mode[i] = 1;
+        if (strip_ok) mode[i] = 1;
         else if (u8ok && fast::morph_fast_args(mask, kw, kh, im.v.cn, im.v.w, ma)) mode[i] = 3;
         if (mode[i] == 0) {
           fallback(i, next[i], nullptr);

@@ -86,7 +86,7 @@ __global__ void __launch_bounds__(Op::kThreads) k_batch(TileQ q, typename Op::Ar
 // Warp-granular queue: every warp claims its own tiles (lane 0 takes the
 // ticket, the warp broadcasts it); no block barrier after the prefix cache.
 template <class Op>
-__global__ void __launch_bounds__(Op::kThreads) k_batch_warp(TileQ q, typename Op::Args a) {
+__global__ void __launch_bounds__(Op::kThreads, Op::kMinBlocks) k_batch_warp(TileQ q, typename Op::Args a) {
   __shared__ int s_start[kStartCap + 1];
   const bool cached = q.n <= kStartCap;
   if (cached)
@@ -334,7 +334,7 @@ struct OpLut {
 // u8 Gaussian with binomial taps on warp strips (strip.cuh).
 template <int K, int CN, int RH>
 struct OpGaussStrip {
-  static constexpr int kThreads = 256;
+  static constexpr int kThreads = 128, kMinBlocks = 4;  // <= 128 registers (no spills)
   static constexpr bool kWarpTiles = true;
   using Args = strip::GaussArgs;
   static size_t smem(const Args &) { return 0; }
@@ -351,7 +351,7 @@ struct NoArgs {
 // on warp strips (strip.cuh).
 template <class P1, class P2, int CN, int RH, bool MAX1, bool FUSED>
 struct OpMorphStrip {
-  static constexpr int kThreads = 256;
+  static constexpr int kThreads = 128, kMinBlocks = FUSED ? 5 : 6;  // 102 / 85 registers
   static constexpr bool kWarpTiles = true;
   using Args = NoArgs;
   static size_t smem(const Args &) { return 0; }

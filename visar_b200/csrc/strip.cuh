@@ -1,9 +1,8 @@
-// Warp-strip stencils for u8 images: a warp owns a strip of 32 four-sample
-// words across RH output rows and walks down it, keeping the vertical window
-// in registers; horizontal neighbours come from the adjacent lanes by warp
-// shuffles. The outer lanes of a strip are halo (loaded, not written), so a
-// strip writes 32 - 2*halo words. No shared memory and no block barriers:
-// each warp streams its own rows, with kBatch row loads in flight.
+// Warp-strip stencils for u8 images: a warp owns a strip of 32 lanes x 8
+// samples across RH output rows and walks down it, keeping the vertical
+// window in registers; horizontal neighbours come from the adjacent lanes by
+// warp shuffles. The outer lanes of a strip are halo (loaded, not written).
+// No shared memory and no block barriers: each warp streams its own rows.
 //
 // Two operations:
 //  * gauss_strip: u8 Gaussian whose fixed-point taps are g * binomial(K)
@@ -19,8 +18,9 @@
 //    native instructions (byte-lane min/max are not). Out-of-image pixels hold
 //    the identity (morph.zig:489-519).
 //
-// Rows stream through a double buffer: the loads of the next kBatch rows are
-// issued before the current kBatch rows are computed.
+// Rows stream through a register queue: the load of row j + kPD is issued
+// when row j is computed, so kPD rows per lane are always in flight, and the
+// row loop stays rolled (small code for the instruction cache).
 #pragma once
 #include "morphfast.cuh"
 #include "vb.h"
@@ -29,58 +29,123 @@ namespace vb {
 namespace strip {
 
 constexpr unsigned kFull = 0xFFFFFFFFu;
-constexpr int kBatch = 8;  // row loads in flight per lane
+constexpr int kPD = 8;   // rows in flight per lane (a register queue)
+constexpr int kSPL = 8;  // samples per lane (one 8-byte word)
 
-// Column description of one lane's word.
+// Column description of one lane's 8 samples. Lanes whose samples are all
+// inside the row load them with one 8-byte load; lanes entirely outside the
+// stencil's reach (REACH samples beyond the row) load nothing; the few lanes
+// that straddle an edge read each sample through an index precomputed once
+// per tile into shared memory: the border map for Gaussian rows (constant
+// border: the fill value), the fill value (identity) for morphology.
 struct Cols {
-  long long gs;  // first sample of the word
-  bool inside;   // all four samples inside the row
-  int msi[4];    // sample index each byte reads (-1: fill value)
+  long long gs;  // first sample of the lane
+  long long n;   // samples per row
+  bool inside;   // all samples inside the row
+  bool edge;     // straddles an edge within reach: indexed loads
+  int *idx;      // this lane's 8 sample indices (-1: fill) when edge
 };
 
-// Gaussian rows: samples outside the row go through the border map (constant
-// border: fill). Morphology (ident): outside samples take the fill value.
-template <int CN>
-__device__ __forceinline__ Cols make_cols(long long gs, long long n, int W, int border, bool ident) {
+// Per-warp index slots for edge lanes: 8 ints per lane, kWarpsPerBlock warps.
+constexpr int kWarpsPerBlock = 4;
+
+template <int CN, int REACH>
+__device__ __forceinline__ Cols make_cols(long long gs, long long n, int W, int border, bool ident, int lane) {
+  __shared__ int s_idx[kWarpsPerBlock][32][kSPL];
   Cols c;
   c.gs = gs;
-  c.inside = gs >= 0 && gs + 4 <= n;
-#pragma unroll
-  for (int k = 0; k < 4; k++) c.msi[k] = -1;
-  if (!c.inside) {
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
+  c.n = n;
+  c.inside = gs >= 0 && gs + kSPL <= n;
+  c.edge = !c.inside && gs + kSPL > -REACH && gs < n + REACH;
+  c.idx = s_idx[(threadIdx.x >> 5) % kWarpsPerBlock][lane];
+  if (c.edge) {
+    for (int k = 0; k < kSPL; k++) {
       const long long g = gs + k;
-      if (ident) {
-        c.msi[k] = (g >= 0 && g < n) ? (int)g : -1;
+      int m;
+      if (g >= 0 && g < n) {
+        m = (int)g;
+      } else if (ident) {
+        m = -1;
       } else {
         const long long px = g >= 0 ? g / CN : -((-g + CN - 1) / CN);
         const int mx = border_map(px, W, border);
-        c.msi[k] = mx < 0 ? -1 : (int)(mx * CN + (g - px * CN));
+        m = mx < 0 ? -1 : (int)(mx * CN + (g - px * CN));
       }
+      c.idx[k] = m;
     }
   }
+  __syncwarp();
   return c;
 }
 
-__device__ __forceinline__ uint32_t load_word(const uint8_t *row, const Cols &c, uint32_t fill) {
-  if (c.inside) return __ldg(reinterpret_cast<const uint32_t *>(row + c.gs));
-  uint32_t w = 0;
+static __device__ __noinline__ uint2 load8_edge(const uint8_t *row, const int *idx, uint32_t fill) {
+  uint32_t v[2] = {0, 0};
 #pragma unroll
-  for (int k = 0; k < 4; k++) {
-    const uint32_t b = c.msi[k] < 0 ? ((fill >> (8 * k)) & 0xFFu) : (uint32_t)__ldg(row + c.msi[k]);
-    w |= b << (8 * k);
+  for (int k = 0; k < kSPL; k++) {
+    const int m = idx[k];
+    const uint32_t b = m < 0 ? (fill & 0xFFu) : (uint32_t)__ldg(row + m);
+    v[k >> 2] |= b << (8 * (k & 3));
   }
-  return w;
+  return make_uint2(v[0], v[1]);
 }
 
-__device__ __forceinline__ void store_word(uint8_t *row, long long gs, long long n, uint32_t w) {
-  if (gs + 4 <= n) {
-    *reinterpret_cast<uint32_t *>(row + gs) = w;
+// The lane's 8 samples of a row (rows 8-byte aligned).
+__device__ __forceinline__ uint2 load8(const uint8_t *row, const Cols &c, uint32_t fill) {
+  if (c.inside) return __ldg(reinterpret_cast<const uint2 *>(row + c.gs));
+  if (c.edge) return load8_edge(row, c.idx, fill);
+  return make_uint2(fill, fill);
+}
+
+__device__ __forceinline__ void store8(uint8_t *row, long long gs, long long n, uint32_t lo, uint32_t hi) {
+  if (gs + kSPL <= n) {
+    *reinterpret_cast<uint2 *>(row + gs) = make_uint2(lo, hi);
   } else {
-    for (int k = 0; k < 4 && gs + k < n; k++) row[gs + k] = (uint8_t)(w >> (8 * k));
+    for (int k = 0; k < kSPL && gs + k < n; k++) row[gs + k] = (uint8_t)((k < 4 ? lo : hi) >> (8 * (k & 3)));
   }
 }
+
+// The four sample pairs (16-bit lanes) of 8 bytes: pairs (0,1) (2,3) (4,5) (6,7).
+__device__ __forceinline__ void unpack_pairs(uint2 v, uint32_t (&p)[4]) {
+  p[0] = __byte_perm(v.x, 0, 0x4140);
+  p[1] = __byte_perm(v.x, 0, 0x4342);
+  p[2] = __byte_perm(v.y, 0, 0x4140);
+  p[3] = __byte_perm(v.y, 0, 0x4342);
+}
+
+// The low bytes of four pair registers as 8 bytes.
+__device__ __forceinline__ uint2 pack_pairs(const uint32_t (&p)[4]) {
+  return make_uint2(__byte_perm(p[0], p[1], 0x6420), __byte_perm(p[2], p[3], 0x6420));
+}
+
+// Sample pairs of this lane and NL neighbour lanes each side, gathered by
+// shuffles: q[4*(l+NL) + i] = pair i of lane (self + l). Only the pairs that
+// samples [S0, S1] (relative to this lane's first sample) touch are fetched.
+template <int NL, int S0, int S1>
+struct Window {
+  static constexpr int NQ = 4 * (2 * NL + 1) + 1;
+  uint32_t q[NQ];
+  __device__ __forceinline__ void gather(const uint32_t (&own)[4]) {
+    constexpr int T0 = S0 + kSPL * NL, T1 = S1 + kSPL * NL;  // sample range in q's frame
+    constexpr int PMIN = T0 >> 1, PMAX = (T1 + 1) >> 1;      // pairs at() can touch
+#pragma unroll
+    for (int i = 0; i < NQ; i++) q[i] = 0;
+#pragma unroll
+    for (int i = 0; i < 4; i++) q[4 * NL + i] = own[i];
+#pragma unroll
+    for (int l = 1; l <= NL; l++)
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        const int il = 4 * (NL - l) + i, ir = 4 * (NL + l) + i;
+        if (il >= PMIN && il <= PMAX) q[il] = __shfl_up_sync(kFull, own[i], l);
+        if (ir >= PMIN && ir <= PMAX) q[ir] = __shfl_down_sync(kFull, own[i], l);
+      }
+  }
+  // (V[s], V[s+1]) for s relative to this lane's first sample.
+  __device__ __forceinline__ uint32_t at(int s) const {
+    const int t = s + kSPL * NL;
+    return (t & 1) ? __byte_perm(q[t >> 1], q[(t >> 1) + 1], 0x5432) : q[t >> 1];
+  }
+};
 
 // ------------------------------------------------------------ Gaussian
 
@@ -95,111 +160,88 @@ struct Binom<5> {
   static constexpr int e = 4;  // g = 16
 };
 
-// Pair (V[s], V[s+1]) in 16-bit lanes, s relative to the lane's word start,
-// from the pairs of words -NW..NW (pq[2*(w+NW)] = samples 0,1 of word w).
-template <int NW>
-__device__ __forceinline__ uint32_t pair_at(const uint32_t *pq, int s) {
-  const int t = s + 4 * NW;
-  return (t & 1) ? __byte_perm(pq[t >> 1], pq[(t >> 1) + 1], 0x5432) : pq[t >> 1];
-}
-
-// Horizontal binomial sums of the two output pairs of this lane's word, from
-// the vertical sums (lo = samples 0,1; hi = samples 2,3) of every lane.
-template <int K, int CN>
-__device__ __forceinline__ void hsum(uint32_t lo, uint32_t hi, uint32_t &h0, uint32_t &h1) {
-  constexpr int R = K / 2;
-  constexpr int NW = (R * CN + 3) / 4;
-  uint32_t pq[2 * (2 * NW + 1) + 1];
-  pq[2 * NW] = lo;
-  pq[2 * NW + 1] = hi;
-#pragma unroll
-  for (int k = 1; k <= NW; k++) {
-    pq[2 * (NW - k)] = __shfl_up_sync(kFull, lo, k);
-    pq[2 * (NW - k) + 1] = __shfl_up_sync(kFull, hi, k);
-    pq[2 * (NW + k)] = __shfl_down_sync(kFull, lo, k);
-    pq[2 * (NW + k) + 1] = __shfl_down_sync(kFull, hi, k);
-  }
-  pq[2 * (2 * NW + 1)] = 0;
-  uint32_t h[2];
-#pragma unroll
-  for (int o = 0; o < 2; o++) {
-    const int c = 2 * o;
-    if constexpr (K == 3) {
-      h[o] = pair_at<NW>(pq, c - CN) + pair_at<NW>(pq, c + CN) + (pair_at<NW>(pq, c) << 1);
-    } else {
-      const uint32_t a = pair_at<NW>(pq, c - 2 * CN) + pair_at<NW>(pq, c + 2 * CN);
-      const uint32_t b = pair_at<NW>(pq, c - CN) + pair_at<NW>(pq, c + CN);
-      h[o] = a + (b << 2) + pair_at<NW>(pq, c) * 6u;
-    }
-  }
-  h0 = h[0];
-  h1 = h[1];
-}
-
 struct GaussArgs {
   int border;
 };
 
-// One strip tile: words [tx*OW - NW, tx*OW - NW + 32) of rows
-// [ty*RH, ty*RH + RH); `lane` is this thread's lane.
+template <int K, int CN>
+struct GaussGeom {
+  static constexpr int R = K / 2;
+  static constexpr int REACH = R * CN;
+  static constexpr int HALO = (REACH + kSPL - 1) / kSPL;  // halo lanes each side
+  static constexpr int OL = 32 - 2 * HALO;                // output lanes
+};
+
+// One strip tile: lanes cover samples [(tx*OL - HALO + lane) * 8, +8) of
+// rows [ty*RH, ty*RH + RH). The vertical binomial runs as a cascade of
+// pairwise sums over the incoming rows; the horizontal one on the pairs of
+// this lane and its neighbours.
 template <int K, int CN, int RH>
 __device__ __forceinline__ void gauss_strip(const DImg &s, const DImg &d, int border, int tx, int ty, int lane) {
-  constexpr int R = K / 2;
-  constexpr int NW = (R * CN + 3) / 4;
-  constexpr int OW = 32 - 2 * NW;
+  using G = GaussGeom<K, CN>;
+  constexpr int R = G::R, HALO = G::HALO;
   constexpr int NR = RH + K - 1;
   constexpr int E = Binom<K>::e;
   constexpr int SH = 16 - 2 * E;
   constexpr uint32_t RND = (1u << (SH - 1)) * 0x00010001u;
   const long long n = (long long)s.w * CN;
-  const long long gw = (long long)tx * OW - NW + lane;
-  const Cols c = make_cols<CN>(gw * 4, n, s.w, border, false);
+  const long long gs = ((long long)tx * G::OL - HALO + lane) * kSPL;
+  const Cols c = make_cols<CN, G::REACH>(gs, n, s.w, border, false, lane);
   const int y0 = ty * RH;
-  const bool out_lane = lane >= NW && lane < 32 - NW && c.gs < n;
-  // Binomial cascade of pairwise sums; after row j the last stage holds the
-  // binomial sum of rows j-K+1..j.
-  uint32_t pl[K - 1], ph[K - 1];
-#pragma unroll
-  for (int k = 0; k < K - 1; k++) pl[k] = ph[k] = 0;
-  auto load_batch = [&](int jb, uint32_t (&w)[kBatch]) {
-#pragma unroll
-    for (int k = 0; k < kBatch; k++) {
-      w[k] = 0;
-      if (jb + k < NR) {
-        const int my = border_map(y0 - R + jb + k, s.h, border);
-        if (my >= 0) w[k] = load_word(row_ptr<const uint8_t>(s, my), c, 0u);
-      }
-    }
+  const bool out_lane = lane >= HALO && lane < 32 - HALO && gs < n;
+  auto load_row = [&](int j) -> uint2 {
+    const int my = border_map(y0 - R + j, s.h, border);
+    return my < 0 ? make_uint2(0, 0) : load8(row_ptr<const uint8_t>(s, my), c, 0u);
   };
-  uint32_t w[kBatch], wn[kBatch];
-  load_batch(0, w);
+  uint2 q[kPD];
+#pragma unroll
+  for (int k = 0; k < kPD; k++) q[k] = make_uint2(0, 0);
+  uint32_t cas[K - 1][4];
+#pragma unroll
+  for (int a = 0; a < K - 1; a++)
+#pragma unroll
+    for (int i = 0; i < 4; i++) cas[a][i] = 0;
+  // The first kPD iterations only fill the queue (one load site, rolled).
 #pragma unroll 1
-  for (int jb = 0; jb < NR; jb += kBatch) {
-    if (jb + kBatch < NR) load_batch(jb + kBatch, wn);
+  for (int j = -kPD; j < NR; j++) {
+    const uint2 cur = q[0];
 #pragma unroll
-    for (int k = 0; k < kBatch; k++) {
-      const int j = jb + k;
-      if (j >= NR) break;
-      uint32_t cl = __byte_perm(w[k], 0, 0x4140), ch = __byte_perm(w[k], 0, 0x4342);
+    for (int k = 0; k < kPD - 1; k++) q[k] = q[k + 1];
+    q[kPD - 1] = j + kPD < NR ? load_row(j + kPD) : make_uint2(0, 0);
+    if (j < 0) continue;
+    // Cascade of pairwise sums: after row j the last stage holds the
+    // binomial sum of rows j-K+1..j.
+    uint32_t v[4];
+    unpack_pairs(cur, v);
 #pragma unroll
-      for (int q = 0; q < K - 1; q++) {
-        const uint32_t nl = cl + pl[q], nh = ch + ph[q];
-        pl[q] = cl;
-        ph[q] = ch;
-        cl = nl;
-        ch = nh;
+    for (int a = 0; a < K - 1; a++)
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        const uint32_t t = v[i] + cas[a][i];
+        cas[a][i] = v[i];
+        v[i] = t;
       }
-      if (j < K - 1) continue;  // window not full yet (warp-uniform)
-      uint32_t h0, h1;
-      hsum<K, CN>(cl, ch, h0, h1);
-      const int y = y0 + j - (K - 1);
-      if (out_lane && y < d.h) {
-        const uint32_t t0 = (h0 + RND) >> SH, t1 = (h1 + RND) >> SH;
-        store_word(row_ptr<uint8_t>(d, y), c.gs, n, __byte_perm(t0, t1, 0x6420));
+    if (j < K - 1) continue;  // window not full yet (warp-uniform)
+    Window<HALO, -G::REACH, kSPL - 1 + G::REACH> win;
+    win.gather(v);
+    uint32_t h[4];
+#pragma unroll
+    for (int o = 0; o < 4; o++) {
+      const int c0 = 2 * o;
+      if constexpr (K == 3) {
+        h[o] = win.at(c0 - CN) + win.at(c0 + CN) + (win.at(c0) << 1);
+      } else {
+        const uint32_t a = win.at(c0 - 2 * CN) + win.at(c0 + 2 * CN);
+        const uint32_t b = win.at(c0 - CN) + win.at(c0 + CN);
+        h[o] = a + (b << 2) + win.at(c0) * 6u;
       }
+      h[o] = (h[o] + RND) >> SH;
     }
-#pragma unroll
-    for (int k = 0; k < kBatch; k++) w[k] = wn[k];
+    const int y = y0 + j - (K - 1);
+    if (out_lane && y < d.h) {
+      const uint2 o8 = pack_pairs(h);
+      store8(row_ptr<uint8_t>(d, y), gs, n, o8.x, o8.y);
+    }
   }
 }
 
@@ -226,83 +268,80 @@ __device__ __forceinline__ uint32_t pop(uint32_t a, uint32_t b) {
   return MAX ? __vmaxu2(a, b) : __vminu2(a, b);
 }
 
-// Runs of every half-width 0..M of the two sample pairs of this lane's word
-// (r[w][0]: samples 0,1; r[w][1]: samples 2,3), from every lane's pairs.
+// Runs of every half-width 0..M over this lane's four pairs.
 template <int M, int CN, bool MAX>
-__device__ __forceinline__ void pair_runs(uint32_t lo, uint32_t hi, uint32_t (&r)[M + 1][2]) {
-  constexpr int NW = (M * CN + 3) / 4;
-  uint32_t pq[2 * (2 * NW + 1) + 1];
-  pq[2 * NW] = lo;
-  pq[2 * NW + 1] = hi;
+__device__ __forceinline__ void pair_runs(const uint32_t (&own)[4], uint32_t (&r)[M + 1][4]) {
+  constexpr int REACH = M * CN;
+  constexpr int NL = (REACH + kSPL - 1) / kSPL;
+  Window<NL, -REACH, kSPL - 1 + REACH> win;
+  win.gather(own);
 #pragma unroll
-  for (int k = 1; k <= NW; k++) {
-    pq[2 * (NW - k)] = __shfl_up_sync(kFull, lo, k);
-    pq[2 * (NW - k) + 1] = __shfl_up_sync(kFull, hi, k);
-    pq[2 * (NW + k)] = __shfl_down_sync(kFull, lo, k);
-    pq[2 * (NW + k) + 1] = __shfl_down_sync(kFull, hi, k);
-  }
-  pq[2 * (2 * NW + 1)] = 0;
-#pragma unroll
-  for (int p = 0; p < 2; p++) {
+  for (int p = 0; p < 4; p++) {
     const int o = 2 * p;
-    r[0][p] = pair_at<NW>(pq, o);
+    r[0][p] = own[p];
 #pragma unroll
-    for (int w = 1; w <= M; w++) r[w][p] = pop<MAX>(r[w - 1][p], pop<MAX>(pair_at<NW>(pq, o - w * CN), pair_at<NW>(pq, o + w * CN)));
+    for (int w = 1; w <= M; w++) r[w][p] = pop<MAX>(r[w - 1][p], pop<MAX>(win.at(o - w * CN), win.at(o + w * CN)));
   }
 }
 
-// Running vertical combination: acc[j] collects output row (r - j + ay)
+// Running vertical combination: a[j] collects output row (r - j + ay)
 // while source row r arrives, from element row j.
 template <class PR, bool MAX>
 struct Acc {
   static constexpr int KH = PR::KH;
   static constexpr uint32_t I = MAX ? 0u : 0x00FF00FFu;
-  uint32_t a[KH][2];
+  uint32_t a[KH][4];
   __device__ __forceinline__ void init() {
 #pragma unroll
-    for (int j = 0; j < KH; j++) a[j][0] = a[j][1] = I;
+    for (int j = 0; j < KH; j++)
+#pragma unroll
+      for (int p = 0; p < 4; p++) a[j][p] = I;
   }
-  // Adds a row of runs; returns the completed output pairs (of row r - (KH-1) + ay).
+  // Adds a row of runs; o receives the completed output row (r - (KH-1) + ay).
   template <int M>
-  __device__ __forceinline__ void add(const uint32_t (&r)[M + 1][2], uint32_t &o0, uint32_t &o1) {
+  __device__ __forceinline__ void add(const uint32_t (&r)[M + 1][4], uint32_t (&o)[4]) {
 #pragma unroll
     for (int j = 0; j < KH; j++) {
       const int dj = PR::at(j);
       if (dj < 0) continue;
-      a[j][0] = pop<MAX>(a[j][0], r[dj][0]);
-      a[j][1] = pop<MAX>(a[j][1], r[dj][1]);
-    }
-    o0 = a[KH - 1][0];
-    o1 = a[KH - 1][1];
 #pragma unroll
-    for (int j = KH - 1; j > 0; j--) {
-      a[j][0] = a[j - 1][0];
-      a[j][1] = a[j - 1][1];
+      for (int p = 0; p < 4; p++) a[j][p] = pop<MAX>(a[j][p], r[dj][p]);
     }
-    a[0][0] = a[0][1] = I;
+#pragma unroll
+    for (int p = 0; p < 4; p++) o[p] = a[KH - 1][p];
+#pragma unroll
+    for (int j = KH - 1; j > 0; j--)
+#pragma unroll
+      for (int p = 0; p < 4; p++) a[j][p] = a[j - 1][p];
+#pragma unroll
+    for (int p = 0; p < 4; p++) a[0][p] = I;
   }
 };
 
-// Pairs of the samples outside the row set to the identity.
-__device__ __forceinline__ void mask_pairs(uint32_t &lo, uint32_t &hi, const Cols &c, uint32_t ident) {
+// Pair lanes of samples outside the row set to the identity.
+__device__ __forceinline__ void mask_pairs(uint32_t (&v)[4], const Cols &c, uint32_t ident) {
   if (c.inside) return;
-  if (c.msi[0] < 0) lo = (lo & 0xFFFF0000u) | (ident & 0xFFFFu);
-  if (c.msi[1] < 0) lo = (lo & 0x0000FFFFu) | (ident & 0xFFFF0000u);
-  if (c.msi[2] < 0) hi = (hi & 0xFFFF0000u) | (ident & 0xFFFFu);
-  if (c.msi[3] < 0) hi = (hi & 0x0000FFFFu) | (ident & 0xFFFF0000u);
+#pragma unroll
+  for (int k = 0; k < kSPL; k++) {
+    const long long g = c.gs + k;
+    if (g < 0 || g >= c.n) {
+      const uint32_t m = (k & 1) ? 0xFFFF0000u : 0x0000FFFFu;
+      v[k >> 1] = (v[k >> 1] & ~m) | (ident & m);
+    }
+  }
 }
 
 // One pass (FUSED = false: extremum MAX1 with element P1) or two fused
 // passes (MAX1 with P1, then !MAX1 with P2) over a strip whose outer HALO
-// lanes are not written. A lane's first-pass value at sample k of its word
-// is exact once the lanes within its reach exist, so HALO words of
+// lanes are not written. A lane's first-pass value at a sample is exact once
+// the samples within its reach exist in the strip, so HALO lanes covering
 // (M1 + M2) * CN samples suffice.
 template <class P1, class P2, int CN, int RH, bool MAX1, bool FUSED>
 struct MorphStrip {
   static constexpr int M1 = P1::maxd(), M2 = FUSED ? P2::maxd() : 0;
   static constexpr int KH1 = P1::KH, KH2 = FUSED ? P2::KH : 1;
-  static constexpr int HALO = ((M1 + M2) * CN + 3) / 4 > 0 ? ((M1 + M2) * CN + 3) / 4 : 1;
-  static constexpr int OW = 32 - 2 * HALO;
+  static constexpr int HALO = ((M1 + M2) * CN + kSPL - 1) / kSPL > 0 ? ((M1 + M2) * CN + kSPL - 1) / kSPL : 1;
+  static constexpr int OL = 32 - 2 * HALO;
   static constexpr int AY1 = KH1 / 2, AY2 = FUSED ? KH2 / 2 : 0;
   static constexpr int NSRC = RH + (KH1 - 1) + (FUSED ? KH2 - 1 : 0);
 
@@ -311,59 +350,63 @@ struct MorphStrip {
     constexpr uint32_t I1 = MAX1 ? 0u : 0xFFFFFFFFu;
     constexpr uint32_t I2p = MAX2 ? 0u : 0x00FF00FFu;
     const long long n = (long long)s.w * CN;
-    const long long gw = (long long)tx * OW - HALO + lane;
-    const Cols c = make_cols<CN>(gw * 4, n, s.w, 0, true);
+    const long long gs = ((long long)tx * OL - HALO + lane) * kSPL;
+    const Cols c = make_cols<CN, (M1 + M2) * CN>(gs, n, s.w, 0, true, lane);
     const int H = s.h;
     const int y0 = ty * RH;
     const int first = y0 - AY2 - AY1;
-    const bool out_lane = lane >= HALO && lane < 32 - HALO && c.gs < n;
+    const bool out_lane = lane >= HALO && lane < 32 - HALO && gs < n;
+    auto load_row = [&](int j) -> uint2 {
+      const int sy = first + j;
+      return (sy < 0 || sy >= H) ? make_uint2(I1, I1) : load8(row_ptr<const uint8_t>(s, sy), c, I1);
+    };
     Acc<P1, MAX1> acc1;
     Acc<P2, MAX2> acc2;
     acc1.init();
     acc2.init();
-    auto load_batch = [&](int jb, uint32_t (&w)[kBatch]) {
+    uint2 q[kPD];
 #pragma unroll
-      for (int k = 0; k < kBatch; k++) {
-        const int sy = first + jb + k;
-        w[k] = I1;
-        if (jb + k < NSRC && sy >= 0 && sy < H) w[k] = load_word(row_ptr<const uint8_t>(s, sy), c, I1);
-      }
-    };
-    uint32_t w[kBatch], wn[kBatch];
-    load_batch(0, w);
+    for (int k = 0; k < kPD; k++) q[k] = make_uint2(I1, I1);
+    // The first kPD iterations only fill the queue (one load site, rolled).
 #pragma unroll 1
-    for (int jb = 0; jb < NSRC; jb += kBatch) {
-      if (jb + kBatch < NSRC) load_batch(jb + kBatch, wn);
+    for (int j = -kPD; j < NSRC; j++) {
+      const uint2 cur = q[0];
 #pragma unroll
-      for (int k = 0; k < kBatch; k++) {
-        const int j = jb + k;
-        if (j >= NSRC) break;
-        uint32_t r1[M1 + 1][2];
-        pair_runs<M1, CN, MAX1>(__byte_perm(w[k], 0, 0x4140), __byte_perm(w[k], 0, 0x4342), r1);
-        uint32_t v0, v1;
-        acc1.template add<M1>(r1, v0, v1);
-        if (j < KH1 - 1) continue;
-        const int y1 = first + j - (KH1 - 1) + AY1;  // first-pass row completed
-        if constexpr (!FUSED) {
-          if (out_lane && y1 < d.h) store_word(row_ptr<uint8_t>(d, y1), c.gs, n, __byte_perm(v0, v1, 0x6420));
+      for (int k = 0; k < kPD - 1; k++) q[k] = q[k + 1];
+      q[kPD - 1] = j + kPD < NSRC ? load_row(j + kPD) : make_uint2(I1, I1);
+      if (j < 0) continue;
+      uint32_t v[4];
+      unpack_pairs(cur, v);
+      uint32_t r1[M1 + 1][4];
+      pair_runs<M1, CN, MAX1>(v, r1);
+      uint32_t o1[4];
+      acc1.template add<M1>(r1, o1);
+      if (j < KH1 - 1) continue;
+      const int y1 = first + j - (KH1 - 1) + AY1;  // first-pass row completed
+      if constexpr (!FUSED) {
+        if (out_lane && y1 < d.h) {
+          const uint2 o8 = pack_pairs(o1);
+          store8(row_ptr<uint8_t>(d, y1), gs, n, o8.x, o8.y);
+        }
+      } else {
+        // First-pass values outside the image are the second pass's identity.
+        if (y1 < 0 || y1 >= H) {
+#pragma unroll
+          for (int p = 0; p < 4; p++) o1[p] = I2p;
         } else {
-          // First-pass values outside the image are the second pass's identity.
-          if (y1 < 0 || y1 >= H) {
-            v0 = v1 = I2p;
-          } else {
-            mask_pairs(v0, v1, c, I2p);
-          }
-          uint32_t r2[M2 + 1][2];
-          pair_runs<M2, CN, MAX2>(v0, v1, r2);
-          uint32_t u0, u1;
-          acc2.template add<M2>(r2, u0, u1);
-          if (j < (KH1 - 1) + (KH2 - 1)) continue;
-          const int y2 = y1 - (KH2 - 1) + AY2;
-          if (out_lane && y2 < d.h) store_word(row_ptr<uint8_t>(d, y2), c.gs, n, __byte_perm(u0, u1, 0x6420));
+          mask_pairs(o1, c, I2p);
+        }
+        uint32_t r2[M2 + 1][4];
+        pair_runs<M2, CN, MAX2>(o1, r2);
+        uint32_t o2[4];
+        acc2.template add<M2>(r2, o2);
+        if (j < (KH1 - 1) + (KH2 - 1)) continue;
+        const int y2 = y1 - (KH2 - 1) + AY2;
+        if (out_lane && y2 < d.h) {
+          const uint2 o8 = pack_pairs(o2);
+          store8(row_ptr<uint8_t>(d, y2), gs, n, o8.x, o8.y);
         }
       }
-#pragma unroll
-      for (int k = 0; k < kBatch; k++) w[k] = wn[k];
     }
   }
 };
