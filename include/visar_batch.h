@@ -37,7 +37,8 @@ enum visar_stage_kind {
     /* visar_morphology: i[0] op, i[1] shape, i[2] kw, i[3] kh, i[4] iterations. */
     VISAR_STAGE_MORPHOLOGY = 3,
     /* visar_resize: i[0] interpolation; d[0] fx, d[1] fy. The destination is
-       (round(width * fx), round(height * fy)), half to even, at least 1 (OpenCV's dsize rule). */
+       (max(1, floor(width * fx)), max(1, floor(height * fy))): for fx = fy = 0.5 the
+       (w // 2, h // 2) halving of VISAR's differential tests (tests/py/test_core_vs_opencv.py:229). */
     VISAR_STAGE_RESIZE = 4,
     /* visar_threshold: i[0] type; d[0] thresh, d[1] maxval. */
     VISAR_STAGE_THRESHOLD = 5,

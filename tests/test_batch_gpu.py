@@ -20,7 +20,7 @@ pytestmark = pytest.mark.gpu
 
 
 def dims_after_resize(h, w, fx, fy):
-    return max(1, round(h * fy)), max(1, round(w * fx))
+    return max(1, int(h * fy)), max(1, int(w * fx))
 
 
 def plain_stage(x, spec):
@@ -177,6 +177,9 @@ def test_tuning_choices_give_identical_results():
         for rows in (8, 16, 32):
             B.tune_set("gauss.u8.c1.k5.rows", rows)
             B.tune_set("gauss.u8.c3.k5.rows", rows)
+            for c in (1, 3):
+                B.tune_set(f"gauss_strip.u8.c{c}.k5.rows", 8 if rows == 8 else 32)
+                B.tune_set(f"morph_strip.u8.c{c}.k5.rows", 8 if rows != 32 else 32)
             for er in (1, 3, 64):
                 for op in ("gray", "half", "linear", "lut"):
                     for c in (0, 1, 3):

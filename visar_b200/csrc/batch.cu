@@ -345,33 +345,56 @@ void set_tiles(const Launch &L, BImg &b) {
 }
 
 // Applies the tuning table to a finished class, then tiles its images.
-void tune_and_tile(Launch &L) {
+long long total_tiles(const Launch &L) {
+  long long t = 0;
+  for (const BImg &b : L.imgs) t += (long long)b.tiles_x * b.tiles_y;
+  return t;
+}
+
+// Applies the tuning table to a finished class, then tiles its images. A
+// tuned value wins; otherwise tile heights shrink until the class has
+// enough tiles to occupy the GPU (single large frames need short tiles,
+// large batches take tall ones, which cut halo re-reads and queue traffic).
+void tune_and_tile(Launch &L, int num_sms) {
   const std::string key = launch_key(L);
   const std::string sc = size_class(L.imgs, L.op);
   auto get = [&](const char *field, int def) {
     return tune_get(key + "." + sc + "." + field, tune_get(key + "." + field, def));
   };
+  auto retile = [&]() {
+    for (BImg &b : L.imgs) set_tiles(L, b);
+  };
+  const int tuned = get("rows", -1);
   switch (L.op) {
-    case kOpGauss: {
-      const int r = get("rows", 16);
-      L.rows = r == 8 || r == 16 || r == 32 ? r : 16;
+    case kOpGauss:
+      L.rows = tuned == 8 || tuned == 16 || tuned == 32 ? tuned : 16;
+      retile();
       break;
-    }
     case kOpGray: case kOpHalf: case kOpLinear: case kOpLut: {
-      const int r = get("rows", 8);
-      L.rows = std::min(std::max(r, 1), 64);
+      // Enough CTA tiles for ~8 per SM.
+      L.rows = tuned > 0 ? std::min(tuned, 64) : 8;
+      retile();
+      while (tuned <= 0 && L.rows > 1 && total_tiles(L) < 8LL * num_sms) {
+        L.rows /= 2;
+        retile();
+      }
       break;
     }
-    case kOpGaussStrip: {
-      const int r = get("rows", 32);
-      L.rows = r == 64 ? 64 : 32;
+    case kOpGaussStrip: case kOpMorphStrip: {
+      // Warp tiles: 32 rows when there are ~8 per resident warp slot, else 8.
+      L.rows = tuned == 8 || tuned == 32 ? tuned : 32;
+      retile();
+      if (tuned <= 0 && total_tiles(L) < 8LL * num_sms * 16) {
+        L.rows = 8;
+        retile();
+      }
       break;
     }
-    case kOpMorphStrip: L.rows = 32; break;
-    default: L.rows = 8;
+    default:
+      L.rows = 8;
+      retile();
   }
   L.per_sm = std::max(0, get("per_sm", 0));
-  for (BImg &b : L.imgs) set_tiles(L, b);
 }
 
 bool u8_aligned4(const DImg &v) { return ((uintptr_t)v.p % 4 == 0) && (v.stride % 4 == 0); }
@@ -545,7 +568,7 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
           if (!B.image(im.v.w, im.v.h, im.v.cn, im.depth, tmp[i][k])) return VISAR_OUT_OF_MEMORY;
       }
       for (Launch &l : ls) {
-        tune_and_tile(l);
+        tune_and_tile(l, B.P.num_sms);
         step.launches.push_back(std::move(l));
       }
       ls.clear();
@@ -568,7 +591,7 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
           u8_bytes(*l, src, dst, 1);
         }
         for (Launch &l : pl) {
-          tune_and_tile(l);
+          tune_and_tile(l, B.P.num_sms);
           step.launches.push_back(std::move(l));
         }
       }
@@ -581,7 +604,7 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
       if (!(fx > 0) || !(fy > 0) || !std::isfinite(fx) || !std::isfinite(fy)) return VISAR_INVALID_ARGUMENT;
       for (size_t i = 0; i < n; i++) {
         const Buf &im = cur[i];
-        const double wd = std::nearbyint((double)im.v.w * fx), hd = std::nearbyint((double)im.v.h * fy);
+        const double wd = std::floor((double)im.v.w * fx), hd = std::floor((double)im.v.h * fy);
         if (wd > 1e9 || hd > 1e9) return VISAR_INVALID_ARGUMENT;
         const int dw = std::max(1, (int)wd), dh = std::max(1, (int)hd);
         if (dw == im.v.w && dh == im.v.h && interp != 4) {
@@ -693,7 +716,7 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
       return VISAR_UNSUPPORTED;
   }
   for (Launch &l : ls) {
-    tune_and_tile(l);
+    tune_and_tile(l, B.P.num_sms);
     step.launches.push_back(std::move(l));
   }
   return VISAR_OK;

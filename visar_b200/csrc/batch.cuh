@@ -454,11 +454,10 @@ cudaError_t launch_morph_strip(const LaunchRun &r, int prof, int cn, int rows, b
 // The morphology strip launches of one channel count (one translation unit
 // each, to spread the compile).
 template <int CN>
-cudaError_t launch_morph_strip_cn(const LaunchRun &r, int prof, bool max1, bool fused, cudaStream_t st);
+cudaError_t launch_morph_strip_cn(const LaunchRun &r, int prof, int rows, bool max1, bool fused, cudaStream_t st);
 
-template <class PR, int CN>
-cudaError_t launch_morph_strip_prof(const LaunchRun &r, bool max1, bool fused, cudaStream_t st) {
-  constexpr int RH = 32;
+template <class PR, int CN, int RH>
+cudaError_t launch_morph_strip_rh(const LaunchRun &r, bool max1, bool fused, cudaStream_t st) {
   const NoArgs a{0};
   if (fused)
     return max1 ? launch_op<OpMorphStrip<PR, PR, CN, RH, true, true>>(r, a, st)
@@ -467,17 +466,23 @@ cudaError_t launch_morph_strip_prof(const LaunchRun &r, bool max1, bool fused, c
               : launch_op<OpMorphStrip<PR, PR, CN, RH, false, false>>(r, a, st);
 }
 
+template <class PR, int CN>
+cudaError_t launch_morph_strip_prof(const LaunchRun &r, int rows, bool max1, bool fused, cudaStream_t st) {
+  return rows == 8 ? launch_morph_strip_rh<PR, CN, 8>(r, max1, fused, st)
+                   : launch_morph_strip_rh<PR, CN, 32>(r, max1, fused, st);
+}
+
 template <int CN>
-cudaError_t launch_morph_strip_cn(const LaunchRun &r, int prof, bool max1, bool fused, cudaStream_t st) {
+cudaError_t launch_morph_strip_cn(const LaunchRun &r, int prof, int rows, bool max1, bool fused, cudaStream_t st) {
   using namespace strip;
   switch (prof) {
-    case kRect3: return launch_morph_strip_prof<ProfRect3, CN>(r, max1, fused, st);
-    case kRect5: return launch_morph_strip_prof<ProfRect5, CN>(r, max1, fused, st);
-    case kRect7: return launch_morph_strip_prof<ProfRect7, CN>(r, max1, fused, st);
-    case kCross3: return launch_morph_strip_prof<ProfCross3, CN>(r, max1, fused, st);
-    case kCross5: return launch_morph_strip_prof<ProfCross5, CN>(r, max1, fused, st);
-    case kEll5: return launch_morph_strip_prof<ProfEll5, CN>(r, max1, fused, st);
-    case kEll7: return launch_morph_strip_prof<ProfEll7, CN>(r, max1, fused, st);
+    case kRect3: return launch_morph_strip_prof<ProfRect3, CN>(r, rows, max1, fused, st);
+    case kRect5: return launch_morph_strip_prof<ProfRect5, CN>(r, rows, max1, fused, st);
+    case kRect7: return launch_morph_strip_prof<ProfRect7, CN>(r, rows, max1, fused, st);
+    case kCross3: return launch_morph_strip_prof<ProfCross3, CN>(r, rows, max1, fused, st);
+    case kCross5: return launch_morph_strip_prof<ProfCross5, CN>(r, rows, max1, fused, st);
+    case kEll5: return launch_morph_strip_prof<ProfEll5, CN>(r, rows, max1, fused, st);
+    case kEll7: return launch_morph_strip_prof<ProfEll7, CN>(r, rows, max1, fused, st);
   }
   return cudaErrorNotSupported;
 }

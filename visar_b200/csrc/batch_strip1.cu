@@ -8,7 +8,7 @@ namespace bt {
 template <int K, int CN>
 static cudaError_t gauss_rows(const LaunchRun &r, int rows, int border, cudaStream_t st) {
   const strip::GaussArgs a{border};
-  if (rows == 64) return launch_op<OpGaussStrip<K, CN, 64>>(r, a, st);
+  if (rows == 8) return launch_op<OpGaussStrip<K, CN, 8>>(r, a, st);
   return launch_op<OpGaussStrip<K, CN, 32>>(r, a, st);
 }
 
@@ -26,14 +26,13 @@ cudaError_t launch_gauss_strip(const LaunchRun &r, int k, int cn, int rows, int 
   return cudaErrorNotSupported;
 }
 
-template cudaError_t launch_morph_strip_cn<1>(const LaunchRun &, int, bool, bool, cudaStream_t);
+template cudaError_t launch_morph_strip_cn<1>(const LaunchRun &, int, int, bool, bool, cudaStream_t);
 
 cudaError_t launch_morph_strip(const LaunchRun &r, int prof, int cn, int rows, bool max1, bool fused, cudaStream_t st) {
-  (void)rows;  // the morphology strips are compiled for 32-row tiles
   switch (cn) {
-    case 1: return launch_morph_strip_cn<1>(r, prof, max1, fused, st);
-    case 3: return launch_morph_strip_cn<3>(r, prof, max1, fused, st);
-    case 4: return launch_morph_strip_cn<4>(r, prof, max1, fused, st);
+    case 1: return launch_morph_strip_cn<1>(r, prof, rows, max1, fused, st);
+    case 3: return launch_morph_strip_cn<3>(r, prof, rows, max1, fused, st);
+    case 4: return launch_morph_strip_cn<4>(r, prof, rows, max1, fused, st);
   }
   return cudaErrorNotSupported;
 }

@@ -4,7 +4,7 @@
 namespace vb {
 namespace bt {
 
-template cudaError_t launch_morph_strip_cn<3>(const LaunchRun &, int, bool, bool, cudaStream_t);
+template cudaError_t launch_morph_strip_cn<3>(const LaunchRun &, int, int, bool, bool, cudaStream_t);
 
 }  // namespace bt
 }  // namespace vb

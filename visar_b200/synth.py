@@ -114,3 +114,58 @@ def base_image_torch(h, w, c=3, nrect=8, seed=0, device="cuda"):
     if c == 1:
         img = img[:, :, 0]
     return img.contiguous()
+
+
+class VideoScene:
+    """The video workload's scene: a diagonal gradient background with
+    per-frame Gaussian noise (sigma 4), and 16 filled rectangles and ellipses
+    (sides uniform 40-400 px, random colours) moving at constant velocities
+    of +-12 px/frame and bouncing off the frame borders. frame(k) renders
+    frame k on the device (u8, H x W x 3)."""
+
+    def __init__(self, h=2160, w=3840, nobj=16, seed=3):
+        rng = np.random.default_rng(seed)
+        self.h, self.w, self.seed = h, w, seed
+        self.objs = []
+        for _ in range(nobj):
+            ow, oh = int(rng.integers(40, 401)), int(rng.integers(40, 401))
+            self.objs.append({
+                "ellipse": bool(rng.integers(0, 2)), "w": ow, "h": oh,
+                "x0": float(rng.uniform(0, max(1, w - ow))), "y0": float(rng.uniform(0, max(1, h - oh))),
+                "vx": float(rng.uniform(-12, 12)), "vy": float(rng.uniform(-12, 12)),
+                "col": rng.integers(0, 256, size=3).astype(np.uint8)})
+        self._bg = None
+
+    @staticmethod
+    def _bounce(p0, v, k, span):
+        # Position after k frames of constant velocity, reflected at 0 and span.
+        if span <= 0:
+            return 0.0
+        p = (p0 + v * k) % (2 * span)
+        return p if p <= span else 2 * span - p
+
+    def frame(self, k, device="cuda"):
+        import torch
+        h, w = self.h, self.w
+        if self._bg is None:
+            yy = torch.arange(h, device=device, dtype=torch.float32)[:, None]
+            xx = torch.arange(w, device=device, dtype=torch.float32)[None, :]
+            self._bg = (xx + yy) * (255.0 / max(1, w + h - 2))
+        g = torch.Generator(device=device)
+        g.manual_seed(self.seed * 100003 + k)
+        noise = torch.randn((h, w, 3), generator=g, device=device, dtype=torch.float32) * 4.0
+        img = (self._bg[:, :, None] + noise).round_().clamp_(0, 255).to(torch.uint8)
+        for o in self.objs:
+            x = int(self._bounce(o["x0"], o["vx"], k, w - o["w"]))
+            y = int(self._bounce(o["y0"], o["vy"], k, h - o["h"]))
+            col = torch.as_tensor(o["col"], device=device)
+            if not o["ellipse"]:
+                img[y:y + o["h"], x:x + o["w"]] = col
+            else:
+                ry, rx = o["h"] / 2.0, o["w"] / 2.0
+                yy = torch.arange(o["h"], device=device, dtype=torch.float32)[:, None] + 0.5 - ry
+                xx = torch.arange(o["w"], device=device, dtype=torch.float32)[None, :] + 0.5 - rx
+                m = (yy / ry) ** 2 + (xx / rx) ** 2 <= 1.0
+                sub = img[y:y + o["h"], x:x + o["w"]]
+                sub[m[:sub.shape[0], :sub.shape[1]]] = col
+        return img.contiguous()
