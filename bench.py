@@ -594,6 +594,103 @@ def reference_video(args):
     }
 
 
+# ------------------------------------------------------------------ served
+
+S_RATES = (500, 2000, 8000, 20000)
+S_CORPUS = 384
+
+
+def served_stage_list(B, r):
+    from visar_b200 import synth
+    out = []
+    for name, p in r["stages"]:
+        if name == "gray":
+            out.append(B.gray())
+        elif name == "gauss":
+            out.append(B.gaussian((5, 5), 0.0, 0.0, 4))
+        elif name == "resize":
+            out.append(B.resize(0.5, 0.5, 1))
+        elif name == "affine":
+            out.append(B.warp_affine(synth.rotation_matrix_2d(r["w"] / 2.0, r["h"] / 2.0, p["angle"], 1.0), 1, 0, 0.0))
+        else:
+            out.append(B.morphology(2, 0, (3, 3), 1))
+    return out
+
+
+def bench_served(args, ctx):
+    torch = ctx.torch
+    import ctypes
+    from visar_b200 import batch as B
+    from visar_b200 import serve as S
+    from visar_b200 import synth
+    from visar_b200 import desc
+    corpus = synth.served_requests(S_CORPUS, seed=4)
+    imgs = [synth.served_image(r) for r in corpus]  # device-resident payloads
+    arrs = [S._stage_array(served_stage_list(B, r)) for r in corpus]
+    descs = [desc(x) for x in imgs]
+    torch.cuda.synchronize()
+    dur = args.duration
+    rng = np.random.default_rng(5)
+    peak, peak_kind = load_peaks()
+    results = []
+    for rate in S_RATES:
+        n = int(rate * dur)
+        t = np.cumsum(rng.exponential(1.0 / rate, size=n))
+        idx = rng.integers(0, S_CORPUS, size=n)
+        reqs = (S.TraceRequest * n)()
+        px = 0
+        for i in range(n):
+            k = int(idx[i])
+            reqs[i].arrival_s = float(t[i])
+            reqs[i].input = descs[k]
+            reqs[i].stages = ctypes.cast(arrs[k][0], ctypes.POINTER(S.Stage))
+            reqs[i].nstages = len(corpus[k]["stages"])
+            px += corpus[k]["h"] * corpus[k]["w"]
+        row = {"rate": rate, "requests": n}
+        for mode, tag in ((S.BATCHED, ""), (S.PLAIN, "plain_")):
+            srv = S.Server(pool_bytes=64 << 30, mode=mode)
+            try:
+                lat = (ctypes.c_double * n)()
+                el = ctypes.c_double()
+                rc = S.lib.visar_server_run_trace(srv._h, reqs, n, lat, ctypes.byref(el))
+                S._check(rc)
+                la = np.array(lat[:n])
+                st = srv.stats()
+            finally:
+                srv.close()
+            row[tag + "gpix_s"] = px / el.value / 1e9
+            row[tag + "p50_ms"] = float(np.percentile(la, 50))
+            row[tag + "p99_ms"] = float(np.percentile(la, 99))
+            row[tag + "elapsed_s"] = el.value
+            if mode == S.BATCHED:
+                row["mean_batch"] = st["mean_batch"]
+                row["rounds"] = st["rounds"]
+                row["launches"] = st["launches"]
+                row["fallback_calls"] = st["fallback_calls"]
+        results.append(row)
+    top = results[-1]
+    return {
+        "metric": METRIC, "value": top["gpix_s"], "unit": "Gpix/s", "n_gpus": ctx.world, "steps": len(S_RATES),
+        "warmup": 0, "ms_per_step": top["elapsed_s"] * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8+f32", "data": "synthetic",
+        "config": {"workload": "served", "rates_req_s": list(S_RATES), "duration_s_per_rate": dur,
+                   "corpus": S_CORPUS, "requests": "px log-uniform 0.1-8.3 MP, aspect 0.5-2, 1|3|4 ch, u8 80% / f32 20%, "
+                   "1-4 stages of gray / gauss 5x5 / resize 0.5 / warpAffine +-30 deg / open 3x3",
+                   "payloads": "device-resident corpus (the request rates exceed PCIe)", "pool_bytes": 64 << 30,
+                   "per_rate": results, "value_is": "Gpix/s at the highest rate; p50/p99 per rate in per_rate"},
+        "e2e": None,
+        "roofline": None,
+        "cpu_baseline": None,
+        "clocks": None,
+        "gpu_launches": int(sum(r["launches"] for r in results)),
+    }
+
+
+def reference_served(args):
+    return {"impl": "reference", "unavailable": "served workload: VISAR has no request server; the oracle port "
+            "timings are in the batched-mixed reference line"}
+
+
 # ------------------------------------------------------------- plain-1080p
 
 W, H = 1920, 1080
@@ -765,7 +862,7 @@ def reference_plain(args):
 # -------------------------------------------------------------------- main
 
 WORKLOADS = {"batched-mixed": (bench_batched, reference_batched), "plain-1080p": (bench_plain, reference_plain),
-             "video-4k": (bench_video, reference_video)}
+             "video-4k": (bench_video, reference_video), "served": (bench_served, reference_served)}
 
 
 def main():
@@ -776,6 +873,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="batched-mixed", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--duration", type=float, default=5.0, help="seconds per arrival rate (served workload)")
     args = ap.parse_args()
     ours, ref = WORKLOADS[args.workload]
     if args.impl == "reference":

@@ -59,22 +59,27 @@ void ck(cudaError_t e) {
 // images (set while validating them), else the thread's current device.
 thread_local int t_hint_dev = -1;
 
+struct DevCtx;
+void record_call_done();
+
 template <class F>
 int guarded(F &&f) {
   t_hint_dev = -1;
+  int rc = VISAR_OK;
   try {
     f();
-    return VISAR_OK;
   } catch (const Fail &e) {
     set_error(e.name);
-    return e.status;
+    rc = e.status;
   } catch (const std::bad_alloc &) {
     set_error("OutOfMemory");
-    return VISAR_OUT_OF_MEMORY;
+    rc = VISAR_OUT_OF_MEMORY;
   } catch (...) {
     set_error("Internal");
-    return VISAR_INTERNAL;
+    rc = VISAR_INTERNAL;
   }
+  record_call_done();
+  return rc;
 }
 
 // -------------------------------------------------------- device context
@@ -89,7 +94,12 @@ enum Slot { kSrc, kDst, kTmp1, kTmp2, kTmp3, kTmp4, kTab1, kTab2, kTab3, kTab4, 
 struct DevCtx {
   bool init = false;
   cudaStream_t own = nullptr;
-  cudaStream_t last = nullptr;
+  // Recorded after every call's work: the next call, on whatever stream,
+  // waits for it on the device, so the shared scratch buffers are never used
+  // by two streams at once. An event (not the last stream's handle) keeps
+  // this safe when the caller destroys a stream it passed in.
+  cudaEvent_t done = nullptr;
+  bool has_done = false;
   DevBuf slot[kNumSlots];
 };
 
@@ -97,6 +107,10 @@ std::mutex g_mu;
 DevCtx g_ctx[64];
 thread_local cudaStream_t t_stream = nullptr;
 thread_local int t_async = 0;
+// The call in progress on this thread (its context and stream), for the
+// completion event guarded() records.
+thread_local DevCtx *t_call_ctx = nullptr;
+thread_local cudaStream_t t_call_st = nullptr;
 int g_threads = 0;
 
 struct Call {
@@ -118,14 +132,25 @@ Call begin_call() {
   DevCtx &c = g_ctx[dev];
   if (!c.init) {
     ck(cudaStreamCreateWithFlags(&c.own, cudaStreamNonBlocking));
+    ck(cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming));
     c.init = true;
   }
   cudaStream_t st = t_stream ? t_stream : c.own;
-  // Scratch buffers are shared by all calls on this device: finish the
-  // previous stream's work before another stream reuses them.
-  if (c.last && c.last != st) ck(cudaStreamSynchronize(c.last));
-  c.last = st;
+  // Scratch buffers are shared by all calls on this device: this call's work
+  // starts after the previous call's, whichever stream that used.
+  if (c.has_done) ck(cudaStreamWaitEvent(st, c.done, 0));
+  t_call_ctx = &c;
+  t_call_st = st;
   return Call{&c, st, dev};
+}
+
+// Marks the end of the thread's call in progress on its stream.
+void record_call_done() {
+  if (!t_call_ctx) return;
+  if (cudaEventRecord(t_call_ctx->done, t_call_st) == cudaSuccess) t_call_ctx->has_done = true;
+  else cudaGetLastError();
+  t_call_ctx = nullptr;
+  t_call_st = nullptr;
 }
 
 void *scratch(Call &call, Slot s, size_t bytes) {
@@ -1037,8 +1062,11 @@ int visar_resize_linear_u8_noalloc(const visar_image *src, const visar_image *ds
     // previous call's stream as begin_call orders calls.
     DevCtx &c = g_ctx[dev];
     const cudaStream_t st = t_stream ? t_stream : c.init ? c.own : cudaStreamLegacy;
-    if (c.last && c.last != st) ck(cudaStreamSynchronize(c.last));
-    c.last = st;
+    if (c.has_done) ck(cudaStreamWaitEvent(st, c.done, 0));
+    if (c.init) {
+      t_call_ctx = &c;
+      t_call_st = st;
+    }
     ck(launch_resize_linear_u8_static(s.dev, d.dev, taps, st));
     ck(cudaGetLastError());
     if (!t_async) ck(cudaStreamSynchronize(st));

@@ -169,3 +169,45 @@ class VideoScene:
                 sub = img[y:y + o["h"], x:x + o["w"]]
                 sub[m[:sub.shape[0], :sub.shape[1]]] = col
         return img.contiguous()
+
+
+SERVED_STAGES = ("gray", "gauss", "resize", "affine", "open")
+
+
+def served_requests(n, seed=4, mp_min=0.1, mp_max=8.3):
+    """The served workload's requests: pixel count log-uniform in
+    [mp_min, mp_max] MP, aspect ratio uniform 0.5-2.0, 1 / 3 / 4 channels,
+    u8 (80%) or f32 N(0,1) (20%), and a pipeline of 1-4 stages drawn
+    uniformly from gray, GaussianBlur 5x5, resize linear 0.5x, warpAffine
+    with a random +-30 degree rotation about the centre, and OPEN 3x3 rect.
+    Returns dicts with h, w, c, dtype ('u8' / 'f32'), seed and stages, each a
+    (name, params) pair."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        px = float(np.exp(rng.uniform(np.log(mp_min * 1e6), np.log(mp_max * 1e6))))
+        aspect = float(rng.uniform(0.5, 2.0))
+        w = max(8, int(round(np.sqrt(px * aspect))))
+        h = max(8, int(round(px / w)))
+        c = int(rng.choice([1, 3, 4]))
+        dtype = "f32" if rng.uniform() < 0.2 else "u8"
+        stages = []
+        for _ in range(int(rng.integers(1, 5))):
+            name = SERVED_STAGES[int(rng.integers(0, len(SERVED_STAGES)))]
+            params = {}
+            if name == "affine":
+                params["angle"] = float(rng.uniform(-30, 30))
+            stages.append((name, params))
+        out.append({"h": h, "w": w, "c": c, "dtype": dtype, "seed": seed * 100003 + k, "stages": stages})
+    return out
+
+
+def served_image(r, device="cuda"):
+    """The input image of a served_requests entry, on the device."""
+    import torch
+    if r["dtype"] == "u8":
+        return base_image_torch(r["h"], r["w"], r["c"], nrect=4, seed=r["seed"], device=device)
+    g = torch.Generator(device=device)
+    g.manual_seed(int(r["seed"]))
+    shape = (r["h"], r["w"]) if r["c"] == 1 else (r["h"], r["w"], r["c"])
+    return torch.randn(shape, generator=g, device=device, dtype=torch.float32)
