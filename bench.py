@@ -239,14 +239,34 @@ def c2_cpu_sample(budget_s, max_images=N_IMAGES):
     return px / dt / 1e9, n, px / 1e6, dt, O.get_num_threads()
 
 
+def tune_workload(args, ctx, workload, images, stages, fill=None):
+    """Loads the workload's tuned launch table (`--tuning`, by default
+    visar_b200/tuned/<workload>.json) when it was written for this device,
+    else runs the autotuner and writes it there. Returns the table."""
+    from visar_b200 import autotune
+    if args.no_tune:
+        return None
+    path = args.tuning or os.path.join(ROOT, "visar_b200", "tuned", f"{workload}.json")
+    log = (lambda m: print(f"[tune {workload}] {m}", file=sys.stderr)) if ctx.rank == 0 else None
+    return autotune.ensure(path, images, stages, workload, fill=fill, log=log)
+
+
 def bench_batched(args, ctx):
     torch, vb = ctx.torch, ctx.vb
     from visar_b200 import batch as B
     from visar_b200 import synth
     shapes = mixed_shapes()
+    bases = [synth.base_image_torch(h, w, c, nrect=8, seed=10_000 + k) for k, (h, w, c) in enumerate(shapes)]
+
+    def fill(p):
+        for k, x in enumerate(bases):
+            p.input(k).copy_(x)
+
+    tuned = tune_workload(args, ctx, "batched-mixed", [(h, w, c, np.uint8) for (h, w, c) in shapes], c2_stages(B),
+                          fill)
     plan = B.Batch([(h, w, c, np.uint8) for (h, w, c) in shapes], c2_stages(B))
-    for k, (h, w, c) in enumerate(shapes):
-        plan.input(k).copy_(synth.base_image_torch(h, w, c, nrect=8, seed=10_000 + k))
+    fill(plan)
+    del bases
     info = plan.info()
     px_step = info["pixels_in"]
     ins = [plan.input(k) for k in range(len(shapes))]
@@ -352,7 +372,7 @@ def bench_batched(args, ctx):
                    "pipeline_gbs": pipeline_gbs, "pipeline_frac": pipeline_gbs / peak,
                    "launches_per_step": info["launches"], "fallback_calls": info["fallback_calls"],
                    "plain_gpix_s": plain, "plain_ms_per_step": p_ms, "speedup_vs_plain": value / plain,
-                   "exec": "one CUDA graph per step (persistent tile-queue kernels)",
+                   "exec": "one CUDA graph per step (persistent tile-queue kernels)", "tuning": tuned,
                    "l2": "inputs (1.2 GB) larger than L2", "parallelism": f"replicas{ctx.world}",
                    "kernels": kernels},
         "e2e": {"value": e2e, "unit": "Gpix/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e_ms},
@@ -402,6 +422,7 @@ def reference_batched(args):
 # ---------------------------------------------------------------- video-4k
 
 V_FRAMES, V_H, V_W = 300, 2160, 3840
+V_INSTANCES = 3
 V_BYTES_PER_FRAME = V_W * V_H * 3 + V_W * V_H + 2 * V_W * V_H + 2 * V_W * V_H + 2 * 2 * V_W * V_H + 2 * V_W * V_H
 
 
@@ -440,23 +461,43 @@ def bench_video(args, ctx):
     scene = synth.VideoScene(V_H, V_W, nobj=16, seed=3)
     frames = [scene.frame(k) for k in range(V_FRAMES)]  # 7.5 GB in HBM, outside timing
     torch.cuda.synchronize()
-    plan = B.Batch([(V_H, V_W, 3, np.uint8)], video_stages(B))
+    tuned = tune_workload(args, ctx, "video-4k", [frames[0]], video_stages(B))
+    # V_INSTANCES graph instances on as many streams take the frames in turn,
+    # so one frame's launches overlap the tails of the previous frame's.
+    plans = [B.Batch([(V_H, V_W, 3, np.uint8)], video_stages(B)) for _ in range(V_INSTANCES)]
+    streams = [torch.cuda.Stream() for _ in plans]
+    plan = plans[0]
     assert plan.info()["fallback_calls"] == 0
     vb.set_async(True)
 
     def frame_step(k):
-        plan.set_input(0, frames[k % V_FRAMES])
-        plan.run_graph()
+        i = k % V_INSTANCES
+        vb.set_stream(streams[i])
+        plans[i].set_input(0, frames[k % V_FRAMES])
+        plans[i].run_graph()
 
-    for k in range(args.warmup):
+    def fork(ev):
+        for s in streams:
+            s.wait_event(ev)
+
+    def join():
+        for s in streams:
+            ctx.stream.wait_stream(s)
+        vb.set_stream(ctx.stream)
+
+    for k in range(max(args.warmup, V_INSTANCES)):
         frame_step(k)
+    join()
+    torch.cuda.synchronize()
     ctx.barrier()
     nf = V_FRAMES
     with Clocks(ctx.dev) as clk:
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev0.record(ctx.stream)
+        fork(ev0)
         for k in range(nf):
             frame_step(k)
+        join()
         ev1.record(ctx.stream)
         torch.cuda.synchronize()
         ms = ev0.elapsed_time(ev1)
@@ -469,7 +510,7 @@ def bench_video(args, ctx):
     outs = [torch.empty((V_H, V_W), dtype=torch.uint8, device="cuda") for _ in range(5)]
     video_plain(vb, frames[(nf - 1) % V_FRAMES], outs)
     torch.cuda.synchronize()
-    if not torch.equal(outs[4], plan.output(0)):
+    if not torch.equal(outs[4], plans[(nf - 1) % V_INSTANCES].output(0)):
         raise AssertionError("video: graph result differs from the per-call pipeline")
 
     # per-call drop-in, same GPU
@@ -508,23 +549,31 @@ def bench_video(args, ctx):
         h = torch.empty((V_H, V_W, 3), dtype=torch.uint8, pin_memory=True).numpy()
         h[...] = frames[k].cpu().numpy()
         hosts.append(h)
-    hout = torch.empty((V_H, V_W), dtype=torch.uint8, pin_memory=True).numpy()
-    # The plan's own input buffer receives the uploads.
-    own = B.Batch([(V_H, V_W, 3, np.uint8)], video_stages(B))
+    houts = [torch.empty((V_H, V_W), dtype=torch.uint8, pin_memory=True).numpy() for _ in range(V_INSTANCES)]
+    # Each instance's own input buffer receives its uploads; instance i's
+    # upload, graph and download are ordered on its stream, and the instances
+    # overlap (copy engines and SMs).
+    owns = [B.Batch([(V_H, V_W, 3, np.uint8)], video_stages(B)) for _ in range(V_INSTANCES)]
 
     def e2e_frame(k):
-        own.upload([hosts[k % nh]])
-        own.run_graph()
-        own.download([hout])
+        i = k % V_INSTANCES
+        vb.set_stream(streams[i])
+        owns[i].upload([hosts[k % nh]])
+        owns[i].run_graph()
+        owns[i].download([houts[i]])
 
-    for k in range(3):
+    for k in range(max(3, V_INSTANCES)):
         e2e_frame(k)
+    join()
+    torch.cuda.synchronize()
     ctx.barrier()
     e_n = 60
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(ctx.stream)
+    fork(e0)
     for k in range(e_n):
         e2e_frame(k)
+    join()
     e1.record(ctx.stream)
     torch.cuda.synchronize()
     e_ms = ctx.max_over_ranks(e0.elapsed_time(e1)) / e_n
@@ -553,7 +602,9 @@ def bench_video(args, ctx):
                    "fps": fps, "hbm_gbs_algorithmic": V_BYTES_PER_FRAME * fps / 1e9,
                    "frac_of_peak": V_BYTES_PER_FRAME * fps / 1e9 / peak, "bytes_per_frame": V_BYTES_PER_FRAME,
                    "plain_fps": plain_fps, "speedup_vs_plain": fps / plain_fps,
-                   "exec": "one CUDA graph per frame; input rebound per frame by a one-thread kernel",
+                   "exec": f"one CUDA graph per frame; input rebound per frame by a one-thread kernel; "
+                           f"{V_INSTANCES} graph instances on {V_INSTANCES} streams take the frames in turn",
+                   "tuning": tuned,
                    "l2": "frames (24.9 MB each, 7.5 GB in all) stream from HBM", "parallelism": f"replicas{ctx.world}",
                    "kernels": kernels},
         "e2e": {"value": V_W * V_H / (e_ms / 1e3) / 1e9 * ctx.world, "unit": "Gpix/s",
@@ -884,6 +935,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="batched-mixed", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="built-in launch defaults instead of the tuned table")
+    ap.add_argument("--tuning", default=None, help="tuned table to load, or to write when it was made elsewhere")
     ap.add_argument("--duration", type=float, default=5.0, help="seconds per arrival rate (served workload)")
     args = ap.parse_args()
     ours, ref = WORKLOADS[args.workload]

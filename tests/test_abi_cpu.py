@@ -107,3 +107,31 @@ def test_no_cpu_fallback_without_gpu():
     with pytest.raises(vb.VisarError) as e:
         vb.gaussian_blur(a, (3, 3), 0)
     assert e.value.status == -6 and e.value.name.startswith("CudaError")
+
+
+def test_tuning_table_reader(tmp_path):
+    """visar_tune_load reads the autotuner's flat JSON (string entries are
+    descriptions and are skipped); NULL restores the built-in defaults."""
+    from visar_b200 import batch as B
+    p = tmp_path / "t.json"
+    p.write_text('{"_device": "NVIDIA B200", "_sms": 148, "_workload": "w",\n'
+                 ' "gauss_strip.u8.c1.k5.L.rows": 32, "gray.u8.c3.k0.M.vec": 8, "x.per_sm": -1}\n')
+    try:
+        B.tune_load(str(p))
+        assert B.tune_get("gauss_strip.u8.c1.k5.L.rows") == 32
+        assert B.tune_get("gray.u8.c3.k0.M.vec") == 8
+        assert B.tune_get("x.per_sm") == -1
+        assert B.tune_get("_sms") == 148
+        assert B.tune_get("_device", 7) == 7
+        B.tune_set("half.u8.c1.k0.S.vec", 8)
+        assert B.tune_get("half.u8.c1.k0.S.vec") == 8
+        B.tune_load(None)
+        assert B.tune_get("gauss_strip.u8.c1.k5.L.rows", -5) == -5
+        bad = tmp_path / "bad.json"
+        bad.write_text('{"a": "unterminated')
+        with pytest.raises(vb.VisarError):
+            B.tune_load(str(bad))
+        with pytest.raises(vb.VisarError):
+            B.tune_load(str(tmp_path / "missing.json"))
+    finally:
+        B.tune_load(None)

@@ -172,20 +172,44 @@ def test_more_images_than_prefix_cache():
 
 
 def test_tuning_choices_give_identical_results():
+    """Every candidate the autotuner may pick (tile rows, samples per thread,
+    CTAs per SM) gives the same bytes."""
+    from visar_b200 import autotune
     imgs = mixed_u8(8, seed=31, wmax=900, hmax=500)
+    specs = C2 + [("thresh", {"t": 128, "m": 255, "type": 0})]
+    plan = check_plan(imgs, specs)
+    keys = sorted({s["name"] for s in plan.launch_stats()})
+    del plan
+    assert {autotune.op_of(k) for k in keys} >= {"gray", "gauss_strip", "morph_strip", "lut"}
     try:
-        for rows in (8, 16, 32):
-            B.tune_set("gauss.u8.c1.k5.rows", rows)
-            B.tune_set("gauss.u8.c3.k5.rows", rows)
-            for c in (1, 3):
-                B.tune_set(f"gauss_strip.u8.c{c}.k5.rows", 8 if rows == 8 else 32)
-                B.tune_set(f"morph_strip.u8.c{c}.k5.rows", 8 if rows != 32 else 32)
-            for er in (1, 3, 64):
-                for op in ("gray", "half", "linear", "lut"):
-                    for c in (0, 1, 3):
-                        B.tune_set(f"{op}.u8.c{c}.k0.rows", er)
-                B.tune_set("morph.u8.c1.k5.per_sm", 1 if er == 1 else 0)
-                check_plan(imgs, C2 + [("thresh", {"t": 128, "m": 255, "type": 0})])
+        for field in autotune.FIELDS:
+            n = max(len(autotune.candidates(k, field)) for k in keys)
+            for i in range(n):
+                B.tune_load(None)
+                for k in keys:
+                    c = autotune.candidates(k, field)
+                    if c:
+                        B.tune_set(f"{k}.{field}", c[i % len(c)])
+                check_plan(imgs, specs)
+    finally:
+        B.tune_load(None)
+
+
+def test_autotune_writes_a_table_the_library_reads(tmp_path):
+    from visar_b200 import autotune
+    imgs = mixed_u8(6, seed=51, wmax=600, hmax=400)
+    path = str(tmp_path / "tune.json")
+    try:
+        table = autotune.ensure(path, imgs, [batch_stage(s) for s in C2], "test-c2", reps=1)
+        doc = autotune.read(path)
+        assert doc["_workload"] == "test-c2" and autotune.matches(doc, "test-c2")
+        for k, v in table.items():
+            cls, field = k.rsplit(".", 1)
+            assert v in autotune.candidates(cls, field), k
+            assert B.tune_get(k) == v
+        check_plan(imgs, C2)
+        # A second call reads the cache instead of tuning again.
+        assert autotune.ensure(path, imgs, [], "test-c2") == table
     finally:
         B.tune_load(None)
 

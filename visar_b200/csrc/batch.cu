@@ -68,25 +68,35 @@ bool parse_tune_json(const std::string &txt, std::map<std::string, int> &out) {
 
 // ----------------------------------------------------------------- plan
 
-std::string size_class(const std::vector<BImg> &imgs, int op) {
-  // Mean destination pixels of the class: S < 0.25 MP <= M < 2 MP <= L.
+// Size class of a launch: mean destination pixels per image, S < 0.25 MP <=
+// M < 2 MP <= L, with "1" appended for a single image (a lone frame needs
+// short tiles to fill the GPU where a batch of the same images does not).
+std::string size_class(const std::vector<BImg> &imgs) {
   double px = 0;
   for (const BImg &b : imgs) px += (double)b.d.w * b.d.h;
   px /= std::max<size_t>(1, imgs.size());
-  (void)op;
-  return px < 250e3 ? "S" : px < 2e6 ? "M" : "L";
-}
-
-std::string launch_key(const Launch &L) {
-  char buf[96];
-  std::snprintf(buf, sizeof(buf), "%s.%s.c%d.k%d", op_name(L.op), L.depth == k32F ? "f32" : "u8", L.cn, L.k);
-  return buf;
+  std::string sc = px < 250e3 ? "S" : px < 2e6 ? "M" : "L";
+  if (imgs.size() == 1) sc += "1";
+  return sc;
 }
 
 const char *launch_suffix(const Launch &L) {
   if (L.op != kOpMorph && L.op != kOpMorphStrip) return "";
   if (L.fused) return L.is_max ? ".close" : ".open";
   return L.is_max ? ".max" : ".min";
+}
+
+// Tuning key of a launch class: op.depth.c<channels>.k<size>, the compiled
+// element profile of a morphology strip, the pass (.min/.max/.open/.close).
+std::string launch_key(const Launch &L) {
+  static const char *const prof[strip::kProfileCount] = {"rect3", "rect5", "rect7", "cross3",
+                                                         "cross5", "ell5", "ell7"};
+  char buf[96];
+  std::snprintf(buf, sizeof(buf), "%s.%s.c%d.k%d%s%s%s", op_name(L.op), L.depth == k32F ? "f32" : "u8", L.cn, L.k,
+                L.op == kOpMorphStrip ? "." : "",
+                L.op == kOpMorphStrip && L.sub >= 0 && L.sub < strip::kProfileCount ? prof[L.sub] : "",
+                launch_suffix(L));
+  return buf;
 }
 
 Launch *class_of(std::vector<Launch> &ls, int op, int depth, int cn, int k, bool is_max, bool fused = false,
@@ -155,6 +165,17 @@ int gauss_tiles_x(int w, int cn, int k) {
   return (int)ceil_div(((long long)w * cn + 3) / 4, 128 - 2 * hw);
 }
 
+// Row-tiled operations (256 threads, P samples per thread): threads per row
+// = the smallest power of two covering the row's units, at most 256.
+void row_tiles(BImg &b, long long units, int P, int rows, int h) {
+  const long long per = ceil_div(units, P);
+  int lg = 0;
+  while (lg < 8 && (1LL << lg) < per) lg++;
+  b.lanes = lg;
+  b.tiles_x = (int)ceil_div(per, 1LL << lg);
+  b.tiles_y = (int)ceil_div(h, (long long)rows * (256 >> lg));
+}
+
 // Tiles per image of an operation, for the launch's tuned parameters.
 void set_tiles(const Launch &L, BImg &b) {
   switch (L.op) {
@@ -166,22 +187,10 @@ void set_tiles(const Launch &L, BImg &b) {
       b.tiles_x = (int)ceil_div(((long long)b.s.w * L.cn + 3) / 4, 126);
       b.tiles_y = (int)ceil_div(b.s.h, 8);
       break;
-    case kOpGray:
-      b.tiles_x = (int)ceil_div(b.s.w, 256 * 16);
-      b.tiles_y = (int)ceil_div(b.s.h, L.rows);
-      break;
-    case kOpHalf:
-      b.tiles_x = (int)ceil_div(b.d.w, 256 * 4);
-      b.tiles_y = (int)ceil_div(b.d.h, L.rows);
-      break;
-    case kOpLinear:
-      b.tiles_x = (int)ceil_div(b.d.w, 256);
-      b.tiles_y = (int)ceil_div(b.d.h, L.rows);
-      break;
-    case kOpLut:
-      b.tiles_x = (int)ceil_div((long long)b.s.w * b.s.cn, 256 * 16);
-      b.tiles_y = (int)ceil_div(b.s.h, L.rows);
-      break;
+    case kOpGray: row_tiles(b, b.s.w, L.vec, L.rows, b.s.h); break;
+    case kOpHalf: row_tiles(b, b.d.w, L.vec, L.rows, b.d.h); break;
+    case kOpLinear: row_tiles(b, b.d.w, 1, L.rows, b.d.h); break;
+    case kOpLut: row_tiles(b, (long long)b.s.w * b.s.cn, L.vec, L.rows, b.s.h); break;
     case kOpGaussStrip: {
       const int halo = ((L.k / 2) * L.cn + strip::kSPL - 1) / strip::kSPL;
       b.tiles_x = (int)ceil_div((long long)b.s.w * L.cn, strip::kSPL * (32 - 2 * halo));
@@ -211,9 +220,10 @@ long long total_tiles(const Launch &L) {
 // large batches take tall ones, which cut halo re-reads and queue traffic).
 void tune_and_tile(Launch &L, int num_sms) {
   const std::string key = launch_key(L);
-  const std::string sc = size_class(L.imgs, L.op);
+  const std::string sc = size_class(L.imgs);
+  L.tkey = key + "." + sc;
   auto get = [&](const char *field, int def) {
-    return tune_get(key + "." + sc + "." + field, tune_get(key + "." + field, def));
+    return tune_get(L.tkey + "." + field, tune_get(key + "." + field, def));
   };
   auto retile = [&]() {
     for (BImg &b : L.imgs) set_tiles(L, b);
@@ -225,6 +235,12 @@ void tune_and_tile(Launch &L, int num_sms) {
       retile();
       break;
     case kOpGray: case kOpHalf: case kOpLinear: case kOpLut: {
+      // Samples per thread (vector width): 8 or 16 bytes for gray and the
+      // LUT, 4 or 8 output pixels for the halving.
+      const int vec = get("vec", -1);
+      if (L.op == kOpHalf) L.vec = vec == 8 ? 8 : 4;
+      else if (L.op == kOpLinear) L.vec = 1;
+      else L.vec = vec == 8 ? 8 : 16;
       // Enough CTA tiles for ~8 per SM.
       L.rows = tuned > 0 ? std::min(tuned, 64) : 8;
       retile();
@@ -662,6 +678,16 @@ cudaError_t run_warp(const Plan &P, const Launch &L, cudaStream_t st) {
   return cudaErrorNotSupported;
 }
 
+template <int PX>
+cudaError_t run_half(const Plan &P, const Launch &L, const RowArgs &ra, cudaStream_t st) {
+  switch (L.cn) {
+    case 1: return run_op<OpHalf<1, PX>>(P, L, ra, st);
+    case 2: return run_op<OpHalf<2, PX>>(P, L, ra, st);
+    case 3: return run_op<OpHalf<3, PX>>(P, L, ra, st);
+    default: return run_op<OpHalf<4, PX>>(P, L, ra, st);
+  }
+}
+
 cudaError_t run_launch(const Plan &P, const Launch &L, cudaStream_t st) {
   if (L.total == 0) return cudaSuccess;
   const RowArgs ra{L.rows};
@@ -673,14 +699,12 @@ cudaError_t run_launch(const Plan &P, const Launch &L, cudaStream_t st) {
       if (L.cn == 1) return run_morph<1>(P, L, st);
       if (L.cn == 3) return run_morph<3>(P, L, st);
       return run_morph<4>(P, L, st);
-    case kOpGray: return L.cn == 3 ? run_op<OpGray<3>>(P, L, ra, st) : run_op<OpGray<4>>(P, L, ra, st);
+    case kOpGray:
+      if (L.vec == 8) return L.cn == 3 ? run_op<OpGray<3, 8>>(P, L, ra, st) : run_op<OpGray<4, 8>>(P, L, ra, st);
+      return L.cn == 3 ? run_op<OpGray<3, 16>>(P, L, ra, st) : run_op<OpGray<4, 16>>(P, L, ra, st);
     case kOpHalf:
-      switch (L.cn) {
-        case 1: return run_op<OpHalf<1>>(P, L, ra, st);
-        case 2: return run_op<OpHalf<2>>(P, L, ra, st);
-        case 3: return run_op<OpHalf<3>>(P, L, ra, st);
-        default: return run_op<OpHalf<4>>(P, L, ra, st);
-      }
+      if (L.vec == 8) return run_half<8>(P, L, ra, st);
+      return run_half<4>(P, L, ra, st);
     case kOpLinear:
       switch (L.cn) {
         case 1: return run_op<OpLinear<1>>(P, L, ra, st);
@@ -688,7 +712,9 @@ cudaError_t run_launch(const Plan &P, const Launch &L, cudaStream_t st) {
         case 3: return run_op<OpLinear<3>>(P, L, ra, st);
         default: return run_op<OpLinear<4>>(P, L, ra, st);
       }
-    case kOpLut: return run_op<OpLut>(P, L, LutArgs{L.rows, L.lut}, st);
+    case kOpLut:
+      if (L.vec == 8) return run_op<OpLut<8>>(P, L, LutArgs{L.rows, L.lut}, st);
+      return run_op<OpLut<16>>(P, L, LutArgs{L.rows, L.lut}, st);
     case kOpWarpAff: return L.depth == k8U ? run_warp<uint8_t, false>(P, L, st) : run_warp<float, false>(P, L, st);
     case kOpWarpPer: return L.depth == k8U ? run_warp<uint8_t, true>(P, L, st) : run_warp<float, true>(P, L, st);
   }
@@ -1069,7 +1095,7 @@ int visar_batch_launch_stat_get(const visar_batch *b, size_t i, visar_batch_laun
     for (const Launch &L : s.launches) {
       if (j++ != i) continue;
       std::memset(out, 0, sizeof(*out));
-      std::snprintf(out->name, sizeof(out->name), "%s%s", launch_key(L).c_str(), launch_suffix(L));
+      std::snprintf(out->name, sizeof(out->name), "%s", L.tkey.c_str());
       out->stage = L.stage;
       out->images = L.imgs.size();
       out->tiles = (size_t)L.total;

@@ -31,6 +31,7 @@ struct BImg {
   float mf[6];          // warpAffine inverse map
   float cv;             // border value as f32
   int wide;             // source rows allow 8-byte loads
+  int lanes;            // row-tiled operations: log2 of the threads per row
 };
 
 struct TileQ {
@@ -52,8 +53,15 @@ __device__ __forceinline__ int find_image(const int *start, int n, int t) {
   return lo;
 }
 
+// Resident CTAs per SM an operation asks the register allocator for
+// (Op::kMinBlocks when it declares one).
+template <class Op, class = void>
+struct MinBlocks : std::integral_constant<int, 1> {};
 template <class Op>
-__global__ void __launch_bounds__(Op::kThreads) k_batch(TileQ q, typename Op::Args a) {
+struct MinBlocks<Op, std::void_t<decltype(Op::kMinBlocks)>> : std::integral_constant<int, Op::kMinBlocks> {};
+
+template <class Op>
+__global__ void __launch_bounds__(Op::kThreads, MinBlocks<Op>::value) k_batch(TileQ q, typename Op::Args a) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int s_start[kStartCap + 1];
   __shared__ int s_tile[2];
@@ -158,103 +166,179 @@ struct OpMorph {
   }
 };
 
-// Row-tiled elementwise operations: a tile is `rows` rows x (kThreads * P) pixels.
+// Row-tiled elementwise operations. A thread owns P consecutive samples of a
+// row. An image's rows are shared out to 2^lanes threads per row (per image:
+// the smallest power of two covering the row, at most the CTA), so a CTA
+// works on kThreads >> lanes rows at once and narrow images do not leave most
+// of its threads idle. A tile is rows * (kThreads >> lanes) image rows by
+// P << lanes samples. Threads walk their rows two at a time, issuing both
+// rows' loads before using either (more bytes in flight per thread).
 struct RowArgs {
   int rows;
+};
+
+struct RowSpan {
+  int x0;    // the thread's first sample in the row
+  int y;     // its first row
+  int yend;  // one past the tile's last row
+  int step;  // rows between the thread's rows
+};
+
+template <int kThreads, int P>
+__device__ __forceinline__ RowSpan row_span(const BImg &im, int rows, int tx, int ty, int h) {
+  const int lg = im.lanes;
+  const int rpp = kThreads >> lg;
+  const int t0 = ty * rows * rpp;
+  RowSpan r;
+  r.x0 = ((tx << lg) + (int)(threadIdx.x & ((1u << lg) - 1))) * P;
+  r.y = t0 + (int)(threadIdx.x >> lg);
+  r.yend = min(h, t0 + rows * rpp);
+  r.step = rpp;
+  return r;
+}
+
+template <int N>
+struct VecOf;
+template <>
+struct VecOf<4> {
+  using T = uint32_t;
+};
+template <>
+struct VecOf<8> {
+  using T = uint2;
+};
+template <>
+struct VecOf<16> {
+  using T = uint4;
+};
+
+// K vectors of N bytes held in registers; byte() and word() take constant
+// indices (after unrolling).
+template <int N, int K>
+struct Vb {
+  using T = typename VecOf<N>::T;
+  T v[K];
+  __device__ __forceinline__ void load(const uint8_t *p) {
+#pragma unroll
+    for (int k = 0; k < K; k++) v[k] = __ldg(reinterpret_cast<const T *>(p) + k);
+  }
+  __device__ __forceinline__ void store(uint8_t *p) const {
+#pragma unroll
+    for (int k = 0; k < K; k++) reinterpret_cast<T *>(p)[k] = v[k];
+  }
+  __device__ __forceinline__ uint32_t byte(int i) const { return reinterpret_cast<const uint8_t *>(v)[i]; }
+  __device__ __forceinline__ uint32_t &word(int i) { return reinterpret_cast<uint32_t *>(v)[i]; }
 };
 
 __device__ __forceinline__ uint32_t gray_px(uint32_t b, uint32_t g, uint32_t r) {
   return (b * kB2G + g * kG2G + r * kR2G + (1u << (kGrayShift - 1))) >> kGrayShift;
 }
 
-// BGR / BGRA -> gray, 16 pixels per thread (color.zig:324-403 arithmetic).
-template <int SCN>
+// BGR / BGRA -> gray (color.zig:324-403 arithmetic), P = 8 or 16 pixels per
+// thread.
+template <int SCN, int P>
 struct OpGray {
-  static constexpr int kThreads = 256, P = 16;
+  static constexpr int kThreads = 256;
   using Args = RowArgs;
   static size_t smem(const Args &) { return 0; }
-  static int tiles_x(int w) { return (int)ceil_div(w, kThreads * P); }
-  static int tiles_y(int h, const Args &a) { return (int)ceil_div(h, a.rows); }
+  static __device__ __forceinline__ void px(const Vb<P, SCN> &in, Vb<P, 1> &out) {
+#pragma unroll
+    for (int q = 0; q < P / 4; q++) {
+      uint32_t w = 0;
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        const int p = q * 4 + i;
+        w |= gray_px(in.byte(p * SCN), in.byte(p * SCN + 1), in.byte(p * SCN + 2)) << (8 * i);
+      }
+      out.word(q) = w;
+    }
+  }
   static __device__ __forceinline__ void tile(const BImg &im, const Args &a, int tx, int ty, unsigned char *) {
-    const int x0 = tx * (kThreads * P) + (int)threadIdx.x * P;
-    if (x0 >= im.s.w) return;
-    const bool full = x0 + P <= im.s.w;
-    for (int r = 0; r < a.rows; r++) {
-      const int y = ty * a.rows + r;
-      if (y >= im.s.h) break;
-      const uint8_t *sp = row_ptr<const uint8_t>(im.s, y) + (long long)x0 * SCN;
-      uint8_t *dp = row_ptr<uint8_t>(im.d, y) + x0;
-      if (full && (((uintptr_t)sp | (uintptr_t)dp) % 16) == 0) {
-        uint4 v[SCN];
-#pragma unroll
-        for (int k = 0; k < SCN; k++) v[k] = reinterpret_cast<const uint4 *>(sp)[k];
-        const uint8_t *b = reinterpret_cast<const uint8_t *>(v);
-        uint32_t o[4];
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-          uint32_t w = 0;
-#pragma unroll
-          for (int i = 0; i < 4; i++) {
-            const int p = q * 4 + i;
-            w |= gray_px(b[p * SCN], b[p * SCN + 1], b[p * SCN + 2]) << (8 * i);
-          }
-          o[q] = w;
-        }
-        *reinterpret_cast<uint4 *>(dp) = make_uint4(o[0], o[1], o[2], o[3]);
+    const RowSpan r = row_span<kThreads, P>(im, a.rows, tx, ty, im.s.h);
+    const int w = im.s.w;
+    if (r.x0 >= w) return;
+    const bool full = r.x0 + P <= w;
+    for (int y = r.y; y < r.yend; y += 2 * r.step) {
+      const int y2 = y + r.step;
+      const bool two = y2 < r.yend;
+      const uint8_t *s0 = row_ptr<const uint8_t>(im.s, y) + (long long)r.x0 * SCN;
+      const uint8_t *s1 = row_ptr<const uint8_t>(im.s, two ? y2 : y) + (long long)r.x0 * SCN;
+      uint8_t *d0 = row_ptr<uint8_t>(im.d, y) + r.x0;
+      uint8_t *d1 = row_ptr<uint8_t>(im.d, two ? y2 : y) + r.x0;
+      if (full && (((uintptr_t)s0 | (uintptr_t)s1 | (uintptr_t)d0 | (uintptr_t)d1) % P) == 0) {
+        Vb<P, SCN> i0, i1;
+        i0.load(s0);
+        i1.load(s1);
+        Vb<P, 1> o0, o1;
+        px(i0, o0);
+        px(i1, o1);
+        o0.store(d0);
+        if (two) o1.store(d1);
       } else {
-        for (int i = 0; i < P && x0 + i < im.s.w; i++) dp[i] = (uint8_t)gray_px(sp[i * SCN], sp[i * SCN + 1], sp[i * SCN + 2]);
+        for (int i = 0; i < P && r.x0 + i < w; i++) {
+          d0[i] = (uint8_t)gray_px(s0[i * SCN], s0[i * SCN + 1], s0[i * SCN + 2]);
+          if (two) d1[i] = (uint8_t)gray_px(s1[i * SCN], s1[i * SCN + 1], s1[i * SCN + 2]);
+        }
       }
     }
   }
 };
 
-// Exact halving (resize_u8.zig:381-447), 4 output pixels per thread.
-template <int CN>
+// Exact halving (resize_u8.zig:381-447), P = 4 or 8 output pixels per thread.
+template <int CN, int P>
 struct OpHalf {
-  static constexpr int kThreads = 256, P = 4;
+  static constexpr int kThreads = 256;
   using Args = RowArgs;
   static size_t smem(const Args &) { return 0; }
-  static int tiles_x(int dw) { return (int)ceil_div(dw, kThreads * P); }
-  static int tiles_y(int dh, const Args &a) { return (int)ceil_div(dh, a.rows); }
+  // Output samples of one output row from its two source rows.
+  static __device__ __forceinline__ void px(const Vb<2 * P, CN> &ra, const Vb<2 * P, CN> &rb, Vb<P, CN> &o) {
+#pragma unroll
+    for (int k = 0; k < P * CN / 4; k++) {
+      uint32_t w = 0;
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const int oi = k * 4 + j;  // output sample index within the P pixels
+        const int p = oi / CN, c = oi % CN;
+        const int i = 2 * p * CN + c;
+        w |= ((ra.byte(i) + ra.byte(i + CN) + rb.byte(i) + rb.byte(i + CN) + 2u) >> 2) << (8 * j);
+      }
+      o.word(k) = w;
+    }
+  }
   static __device__ __forceinline__ void tile(const BImg &im, const Args &a, int tx, int ty, unsigned char *) {
-    const int x0 = tx * (kThreads * P) + (int)threadIdx.x * P;
-    if (x0 >= im.d.w) return;
-    const bool full = x0 + P <= im.d.w;
-    for (int r = 0; r < a.rows; r++) {
-      const int y = ty * a.rows + r;
-      if (y >= im.d.h) break;
-      const uint8_t *ra = row_ptr<const uint8_t>(im.s, 2LL * y) + (size_t)x0 * 2 * CN;
-      const uint8_t *rb = row_ptr<const uint8_t>(im.s, 2LL * y + 1) + (size_t)x0 * 2 * CN;
-      uint8_t *o = row_ptr<uint8_t>(im.d, y) + (size_t)x0 * CN;
-      if (full && (((uintptr_t)ra | (uintptr_t)rb) % 8) == 0 && ((uintptr_t)o % 4) == 0) {
-        uint2 va[CN], vb2[CN];
-#pragma unroll
-        for (int k = 0; k < CN; k++) {
-          va[k] = reinterpret_cast<const uint2 *>(ra)[k];
-          vb2[k] = reinterpret_cast<const uint2 *>(rb)[k];
-        }
-        const uint8_t *ba = reinterpret_cast<const uint8_t *>(va);
-        const uint8_t *bb = reinterpret_cast<const uint8_t *>(vb2);
-        uint32_t out[CN];
-#pragma unroll
-        for (int k = 0; k < CN; k++) {
-          uint32_t w = 0;
-#pragma unroll
-          for (int j = 0; j < 4; j++) {
-            const int oi = k * 4 + j;  // output sample index within the 4 pixels
-            const int p = oi / CN, c = oi % CN;
-            const int i = 2 * p * CN + c;
-            w |= (((uint32_t)ba[i] + ba[i + CN] + bb[i] + bb[i + CN] + 2u) >> 2) << (8 * j);
-          }
-          out[k] = w;
-        }
-#pragma unroll
-        for (int k = 0; k < CN; k++) reinterpret_cast<uint32_t *>(o)[k] = out[k];
+    const RowSpan r = row_span<kThreads, P>(im, a.rows, tx, ty, im.d.h);
+    const int dw = im.d.w;
+    if (r.x0 >= dw) return;
+    const bool full = r.x0 + P <= dw;
+    const size_t xs = (size_t)r.x0 * 2 * CN;
+    for (int y = r.y; y < r.yend; y += 2 * r.step) {
+      const int y2 = y + r.step;
+      const bool two = y2 < r.yend;
+      const int yb = two ? y2 : y;
+      const uint8_t *a0 = row_ptr<const uint8_t>(im.s, 2LL * y) + xs;
+      const uint8_t *b0 = row_ptr<const uint8_t>(im.s, 2LL * y + 1) + xs;
+      const uint8_t *a1 = row_ptr<const uint8_t>(im.s, 2LL * yb) + xs;
+      const uint8_t *b1 = row_ptr<const uint8_t>(im.s, 2LL * yb + 1) + xs;
+      uint8_t *o0 = row_ptr<uint8_t>(im.d, y) + (size_t)r.x0 * CN;
+      uint8_t *o1 = row_ptr<uint8_t>(im.d, yb) + (size_t)r.x0 * CN;
+      if (full && (((uintptr_t)a0 | (uintptr_t)b0 | (uintptr_t)a1 | (uintptr_t)b1) % (2 * P)) == 0 &&
+          (((uintptr_t)o0 | (uintptr_t)o1) % P) == 0) {
+        Vb<2 * P, CN> va0, vb0, va1, vb1;
+        va0.load(a0);
+        vb0.load(b0);
+        va1.load(a1);
+        vb1.load(b1);
+        Vb<P, CN> w0, w1;
+        px(va0, vb0, w0);
+        px(va1, vb1, w1);
+        w0.store(o0);
+        if (two) w1.store(o1);
       } else {
-        for (int p = 0; p < P && x0 + p < im.d.w; p++)
+        for (int p = 0; p < P && r.x0 + p < dw; p++)
           for (int c = 0; c < CN; c++) {
             const int i = 2 * p * CN + c;
-            o[p * CN + c] = (uint8_t)(((uint32_t)ra[i] + ra[i + CN] + rb[i] + rb[i + CN] + 2u) >> 2);
+            o0[p * CN + c] = (uint8_t)(((uint32_t)a0[i] + a0[i + CN] + b0[i] + b0[i + CN] + 2u) >> 2);
+            if (two) o1[p * CN + c] = (uint8_t)(((uint32_t)a1[i] + a1[i + CN] + b1[i] + b1[i + CN] + 2u) >> 2);
           }
       }
     }
@@ -262,33 +346,52 @@ struct OpHalf {
 };
 
 // OpenCV's fixed-point bilinear for u8 (resize_u8.zig:651-711) from the
-// image's tap tables (t0: x taps in pixels, t1: y taps in rows).
+// image's tap tables (t0: x taps in pixels, t1: y taps in rows); one output
+// pixel per thread, two output rows (four source rows) in flight.
 template <int CN>
 struct OpLinear {
-  static constexpr int kThreads = 256, P = 1;
+  static constexpr int kThreads = 256;
   using Args = RowArgs;
   static size_t smem(const Args &) { return 0; }
-  static int tiles_x(int dw) { return (int)ceil_div(dw, kThreads); }
-  static int tiles_y(int dh, const Args &a) { return (int)ceil_div(dh, a.rows); }
   static __device__ __forceinline__ void tile(const BImg &im, const Args &a, int tx, int ty, unsigned char *) {
-    const int x = tx * kThreads + (int)threadIdx.x;
+    const RowSpan r = row_span<kThreads, 1>(im, a.rows, tx, ty, im.d.h);
+    const int x = r.x0;
     if (x >= im.d.w) return;
     const int4 tq = reinterpret_cast<const int4 *>(im.t0)[x];
     const LinTap *yt = static_cast<const LinTap *>(im.t1);
     const int a0 = tq.x * CN, a1 = tq.y * CN;
-    for (int r = 0; r < a.rows; r++) {
-      const int y = ty * a.rows + r;
-      if (y >= im.d.h) break;
-      const LinTap ty2 = yt[y];
-      const uint8_t *r0 = row_ptr<const uint8_t>(im.s, ty2.o0);
-      const uint8_t *r1 = row_ptr<const uint8_t>(im.s, ty2.o1);
-      uint8_t *o = row_ptr<uint8_t>(im.d, y) + (size_t)x * CN;
+    for (int y = r.y; y < r.yend; y += 2 * r.step) {
+      const int y2 = y + r.step;
+      const bool two = y2 < r.yend;
+      const LinTap t0 = yt[y], t1 = yt[two ? y2 : y];
+      const uint8_t *r00 = row_ptr<const uint8_t>(im.s, t0.o0), *r01 = row_ptr<const uint8_t>(im.s, t0.o1);
+      const uint8_t *r10 = row_ptr<const uint8_t>(im.s, t1.o0), *r11 = row_ptr<const uint8_t>(im.s, t1.o1);
+      uint32_t v[4][2][CN];
 #pragma unroll
       for (int c = 0; c < CN; c++) {
-        const int h0 = ((int)r0[a0 + c] * tq.z + (int)r0[a1 + c] * tq.w) >> 4;
-        const int h1 = ((int)r1[a0 + c] * tq.z + (int)r1[a1 + c] * tq.w) >> 4;
-        const int t = ((h0 * ty2.w0) >> 16) + ((h1 * ty2.w1) >> 16);
-        o[c] = (uint8_t)min(max((t + 2) >> 2, 0), 255);
+        v[0][0][c] = __ldg(r00 + a0 + c);
+        v[0][1][c] = __ldg(r00 + a1 + c);
+        v[1][0][c] = __ldg(r01 + a0 + c);
+        v[1][1][c] = __ldg(r01 + a1 + c);
+        v[2][0][c] = __ldg(r10 + a0 + c);
+        v[2][1][c] = __ldg(r10 + a1 + c);
+        v[3][0][c] = __ldg(r11 + a0 + c);
+        v[3][1][c] = __ldg(r11 + a1 + c);
+      }
+      uint8_t *o0 = row_ptr<uint8_t>(im.d, y) + (size_t)x * CN;
+      uint8_t *o1 = row_ptr<uint8_t>(im.d, two ? y2 : y) + (size_t)x * CN;
+#pragma unroll
+      for (int c = 0; c < CN; c++) {
+        const int h00 = ((int)v[0][0][c] * tq.z + (int)v[0][1][c] * tq.w) >> 4;
+        const int h01 = ((int)v[1][0][c] * tq.z + (int)v[1][1][c] * tq.w) >> 4;
+        const int u0 = ((h00 * t0.w0) >> 16) + ((h01 * t0.w1) >> 16);
+        o0[c] = (uint8_t)min(max((u0 + 2) >> 2, 0), 255);
+        if (two) {
+          const int h10 = ((int)v[2][0][c] * tq.z + (int)v[2][1][c] * tq.w) >> 4;
+          const int h11 = ((int)v[3][0][c] * tq.z + (int)v[3][1][c] * tq.w) >> 4;
+          const int u1 = ((h10 * t1.w0) >> 16) + ((h11 * t1.w1) >> 16);
+          o1[c] = (uint8_t)min(max((u1 + 2) >> 2, 0), 255);
+        }
       }
     }
   }
@@ -299,33 +402,50 @@ struct LutArgs {
   const uint8_t *lut;
 };
 
-// u8 threshold through a 256-entry table (threshold.zig:39-60), 16 samples per thread.
+// u8 threshold through a 256-entry table (threshold.zig:39-60), P = 8 or 16
+// samples per thread.
+template <int P>
 struct OpLut {
-  static constexpr int kThreads = 256, P = 16;
+  static constexpr int kThreads = 256;
   using Args = LutArgs;
   static size_t smem(const Args &) { return 256; }
-  static int tiles_x(long long n) { return (int)ceil_div(n, kThreads * P); }
-  static int tiles_y(int h, const Args &a) { return (int)ceil_div(h, a.rows); }
   static __device__ __forceinline__ void tile(const BImg &im, const Args &a, int tx, int ty, unsigned char *smem) {
     uint8_t *t = smem;
     t[threadIdx.x] = a.lut[threadIdx.x];
     __syncthreads();
+    const RowSpan r = row_span<kThreads, P>(im, a.rows, tx, ty, im.s.h);
     const long long n = (long long)im.s.w * im.s.cn;
-    const long long i0 = (long long)tx * (kThreads * P) + threadIdx.x * P;
-    if (i0 >= n) return;
-    for (int r = 0; r < a.rows; r++) {
-      const int y = ty * a.rows + r;
-      if (y >= im.s.h) break;
-      const uint8_t *sp = row_ptr<const uint8_t>(im.s, y) + i0;
-      uint8_t *dp = row_ptr<uint8_t>(im.d, y) + i0;
-      if (i0 + P <= n && (((uintptr_t)sp | (uintptr_t)dp) % 16) == 0) {
-        uint4 v = *reinterpret_cast<const uint4 *>(sp);
-        uint8_t *b = reinterpret_cast<uint8_t *>(&v);
+    if (r.x0 >= n) return;
+    const bool full = r.x0 + P <= n;
+    for (int y = r.y; y < r.yend; y += 2 * r.step) {
+      const int y2 = y + r.step;
+      const bool two = y2 < r.yend;
+      const uint8_t *s0 = row_ptr<const uint8_t>(im.s, y) + r.x0;
+      const uint8_t *s1 = row_ptr<const uint8_t>(im.s, two ? y2 : y) + r.x0;
+      uint8_t *d0 = row_ptr<uint8_t>(im.d, y) + r.x0;
+      uint8_t *d1 = row_ptr<uint8_t>(im.d, two ? y2 : y) + r.x0;
+      if (full && (((uintptr_t)s0 | (uintptr_t)s1 | (uintptr_t)d0 | (uintptr_t)d1) % P) == 0) {
+        Vb<P, 1> v0, v1;
+        v0.load(s0);
+        v1.load(s1);
 #pragma unroll
-        for (int k = 0; k < P; k++) b[k] = t[b[k]];
-        *reinterpret_cast<uint4 *>(dp) = v;
+        for (int q = 0; q < P / 4; q++) {
+          uint32_t w0 = 0, w1 = 0;
+#pragma unroll
+          for (int i = 0; i < 4; i++) {
+            w0 |= (uint32_t)t[v0.byte(q * 4 + i)] << (8 * i);
+            w1 |= (uint32_t)t[v1.byte(q * 4 + i)] << (8 * i);
+          }
+          v0.word(q) = w0;
+          v1.word(q) = w1;
+        }
+        v0.store(d0);
+        if (two) v1.store(d1);
       } else {
-        for (long long k = 0; k < P && i0 + k < n; k++) dp[k] = t[sp[k]];
+        for (long long k = 0; k < P && r.x0 + k < n; k++) {
+          d0[k] = t[s0[k]];
+          if (two) d1[k] = t[s1[k]];
+        }
       }
     }
   }
@@ -334,7 +454,7 @@ struct OpLut {
 // u8 Gaussian with binomial taps on warp strips (strip.cuh).
 template <int K, int CN, int RH>
 struct OpGaussStrip {
-  static constexpr int kThreads = 128, kMinBlocks = 4;  // <= 128 registers (no spills)
+  static constexpr int kThreads = 128, kMinBlocks = 6;  // <= 85 registers (no spills)
   static constexpr bool kWarpTiles = true;
   using Args = strip::GaussArgs;
   static size_t smem(const Args &) { return 0; }

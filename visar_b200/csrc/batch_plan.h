@@ -46,6 +46,7 @@ struct Launch {
   bool is_max = false;
   int rows = 8;     // tile rows (Gaussian band height, elementwise rows)
   int per_sm = 0;   // CTAs per SM (0: as many as fit)
+  int vec = 16;     // row-tiled operations: samples (pixels) per thread
   fast::FastArgs fa{};
   fast::MFArgs ma{};
   bool fused = false;
@@ -58,6 +59,7 @@ struct Launch {
   size_t bytes = 0;  // algorithmic bytes
   int stage = 0;
   mutable int grid = 0;
+  std::string tkey;  // tuning key with the size class (launch_key + ".S|M|L")
   BImg *d_imgs = nullptr;
   int *d_start = nullptr;
   int total = 0;

@@ -9,6 +9,7 @@ template <int K, int CN>
 static cudaError_t gauss_rows(const LaunchRun &r, int rows, int border, cudaStream_t st) {
   const strip::GaussArgs a{border};
   if (rows == 8) return launch_op<OpGaussStrip<K, CN, 8>>(r, a, st);
+  if (rows == 64) return launch_op<OpGaussStrip<K, CN, 64>>(r, a, st);
   return launch_op<OpGaussStrip<K, CN, 32>>(r, a, st);
 }
 

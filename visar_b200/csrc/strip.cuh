@@ -18,10 +18,13 @@
 //    native instructions (byte-lane min/max are not). Out-of-image pixels hold
 //    the identity (morph.zig:489-519).
 //
-// Rows stream through a register queue: the load of row j + kPD is issued
-// when row j is computed, so kPD rows per lane are always in flight, and the
-// row loop stays rolled (small code for the instruction cache).
+// Rows stream through a per-lane queue in shared memory: the copy of row
+// j + kQD (cp.async) is issued when row j is computed, so kQD rows per lane
+// are always in flight. State that moves down with the rows (the Gaussian
+// cascade, the morphology accumulators) alternates between register sets
+// across an unrolled row loop instead of being moved.
 #pragma once
+#include <utility>
 #include "morphfast.cuh"
 #include "vb.h"
 
@@ -29,7 +32,6 @@ namespace vb {
 namespace strip {
 
 constexpr unsigned kFull = 0xFFFFFFFFu;
-constexpr int kPD = 8;   // rows in flight per lane (a register queue)
 constexpr int kSPL = 8;  // samples per lane (one 8-byte word)
 
 // Column description of one lane's 8 samples. Lanes whose samples are all
@@ -87,13 +89,6 @@ static __device__ __noinline__ uint2 load8_edge(const uint8_t *row, const int *i
     v[k >> 2] |= b << (8 * (k & 3));
   }
   return make_uint2(v[0], v[1]);
-}
-
-// The lane's 8 samples of a row (rows 8-byte aligned).
-__device__ __forceinline__ uint2 load8(const uint8_t *row, const Cols &c, uint32_t fill) {
-  if (c.inside) return __ldg(reinterpret_cast<const uint2 *>(row + c.gs));
-  if (c.edge) return load8_edge(row, c.idx, fill);
-  return make_uint2(fill, fill);
 }
 
 __device__ __forceinline__ void store8(uint8_t *row, long long gs, long long n, uint32_t lo, uint32_t hi) {
@@ -172,43 +167,101 @@ struct GaussGeom {
   static constexpr int OL = 32 - 2 * HALO;                // output lanes
 };
 
+// Row queue in shared memory. Each lane copies its 8 samples of source row
+// j + kQD into slot (j + kQD) % kQD with cp.async while row j is computed, so
+// kQD rows per lane are in flight without a register queue to rotate. Lanes
+// that straddle an edge (gathers) or lie outside the row (fill) store their
+// bytes into the slot directly. Slots are lane-private: no barriers.
+constexpr int kQD = 8;
+
+__device__ __forceinline__ void cp_async8(uint32_t saddr, const void *g) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(saddr), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ void st_shared8(uint32_t saddr, uint2 v) {
+  asm volatile("st.shared.v2.u32 [%0], {%1, %2};\n" ::"r"(saddr), "r"(v.x), "r"(v.y) : "memory");
+}
+__device__ __forceinline__ uint2 ld_shared8(uint32_t saddr) {
+  uint2 v;
+  asm volatile("ld.shared.v2.u32 {%0, %1}, [%2];\n" : "=r"(v.x), "=r"(v.y) : "r"(saddr) : "memory");
+  return v;
+}
+
+struct RowQueue {
+  uint32_t base;  // shared address of this lane's bytes in slot 0
+  __device__ __forceinline__ uint32_t slot(int j) const { return base + (uint32_t)((j & (kQD - 1)) * 32 * kSPL); }
+};
+
+__device__ __forceinline__ RowQueue row_queue(int lane) {
+  __shared__ __align__(16) uint2 s_q[kWarpsPerBlock][kQD][32];
+  return RowQueue{(uint32_t)__cvta_generic_to_shared(&s_q[(threadIdx.x >> 5) % kWarpsPerBlock][0][lane])};
+}
+
+// Starts filling a slot with this lane's 8 samples of `row` (nullptr: the
+// fill value everywhere).
+__device__ __forceinline__ void fetch8(uint32_t saddr, const uint8_t *row, const Cols &c, uint32_t fill) {
+  if (row != nullptr && c.inside) cp_async8(saddr, row + c.gs);
+  else if (row != nullptr && c.edge) st_shared8(saddr, load8_edge(row, c.idx, fill));
+  else st_shared8(saddr, make_uint2(fill, fill));
+}
+
 // One strip tile: lanes cover samples [(tx*OL - HALO + lane) * 8, +8) of
 // rows [ty*RH, ty*RH + RH). The vertical binomial runs as a cascade of
-// pairwise sums over the incoming rows; the horizontal one on the pairs of
-// this lane and its neighbours.
+// pairwise sums over the incoming rows (its state alternates between two
+// register sets, ca and cb, so consecutive rows need no moves); the
+// horizontal one on the pairs of this lane and its neighbours.
 template <int K, int CN, int RH>
-__device__ __forceinline__ void gauss_strip(const DImg &s, const DImg &d, int border, int tx, int ty, int lane) {
+struct GaussStrip {
   using G = GaussGeom<K, CN>;
-  constexpr int R = G::R, HALO = G::HALO;
-  constexpr int NR = RH + K - 1;
-  constexpr int E = Binom<K>::e;
-  constexpr int SH = 16 - 2 * E;
-  constexpr uint32_t RND = (1u << (SH - 1)) * 0x00010001u;
-  const long long n = (long long)s.w * CN;
-  const long long gs = ((long long)tx * G::OL - HALO + lane) * kSPL;
-  const Cols c = make_cols<CN, G::REACH>(gs, n, s.w, border, false, lane);
-  const int y0 = ty * RH;
-  const bool out_lane = lane >= HALO && lane < 32 - HALO && gs < n;
-  auto load_row = [&](int j) -> uint2 {
-    const int my = border_map(y0 - R + j, s.h, border);
-    return my < 0 ? make_uint2(0, 0) : load8(row_ptr<const uint8_t>(s, my), c, 0u);
-  };
-  uint2 q[kPD];
-#pragma unroll
-  for (int k = 0; k < kPD; k++) q[k] = make_uint2(0, 0);
-  uint32_t cas[K - 1][4];
-#pragma unroll
-  for (int a = 0; a < K - 1; a++)
-#pragma unroll
-    for (int i = 0; i < 4; i++) cas[a][i] = 0;
-  // The first kPD iterations only fill the queue (one load site, rolled).
-#pragma unroll 1
-  for (int j = -kPD; j < NR; j++) {
-    const uint2 cur = q[0];
-#pragma unroll
-    for (int k = 0; k < kPD - 1; k++) q[k] = q[k + 1];
-    q[kPD - 1] = j + kPD < NR ? load_row(j + kPD) : make_uint2(0, 0);
-    if (j < 0) continue;
+  static constexpr int R = G::R, HALO = G::HALO;
+  static constexpr int NR = RH + K - 1;
+  static constexpr int E = Binom<K>::e;
+  static constexpr int SH = 16 - 2 * E;
+  static constexpr uint32_t RND = (1u << (SH - 1)) * 0x00010001u;
+  static_assert(NR % 2 == 0, "rows per tile plus the stencil's halo must be even");
+
+  const DImg &s, &d;
+  int border, y0;
+  long long n, gs;
+  bool out_lane;
+  Cols c;
+  RowQueue q;
+  uint32_t ca[K - 1][4], cb[K - 1][4];
+
+  __device__ __forceinline__ GaussStrip(const DImg &s_, const DImg &d_, int border_, int tx, int ty, int lane)
+      : s(s_), d(d_), border(border_), y0(ty * RH) {
+    n = (long long)s.w * CN;
+    gs = ((long long)tx * G::OL - HALO + lane) * kSPL;
+    c = make_cols<CN, G::REACH>(gs, n, s.w, border, false, lane);
+    out_lane = lane >= HALO && lane < 32 - HALO && gs < n;
+    q = row_queue(lane);
+  }
+
+  // Source row j of the tile (image row y0 - R + j, border-mapped) into its slot.
+  __device__ __forceinline__ void fetch(int j) {
+    const int sy = y0 - R + j;
+    const uint8_t *row = nullptr;
+    if (sy >= 0 && sy < s.h) {
+      row = row_ptr<const uint8_t>(s, sy);
+    } else {
+      const int my = border_map(sy, s.h, border);
+      if (my >= 0) row = row_ptr<const uint8_t>(s, my);
+    }
+    fetch8(q.slot(j), row, c, 0u);
+  }
+
+  template <bool ODD>
+  __device__ __forceinline__ void step(int j) {
+    const uint32_t(&in)[K - 1][4] = ODD ? cb : ca;
+    uint32_t(&out)[K - 1][4] = ODD ? ca : cb;
+    cp_wait<kQD - 1>();  // row j has landed
+    const uint2 cur = ld_shared8(q.slot(j));
+    if (j + kQD < NR) fetch(j + kQD);
+    cp_commit();
     // Cascade of pairwise sums: after row j the last stage holds the
     // binomial sum of rows j-K+1..j.
     uint32_t v[4];
@@ -217,11 +270,11 @@ __device__ __forceinline__ void gauss_strip(const DImg &s, const DImg &d, int bo
     for (int a = 0; a < K - 1; a++)
 #pragma unroll
       for (int i = 0; i < 4; i++) {
-        const uint32_t t = v[i] + cas[a][i];
-        cas[a][i] = v[i];
+        const uint32_t t = v[i] + in[a][i];
+        out[a][i] = v[i];
         v[i] = t;
       }
-    if (j < K - 1) continue;  // window not full yet (warp-uniform)
+    if (j < K - 1) return;  // window not full yet (warp-uniform)
     Window<HALO, -G::REACH, kSPL - 1 + G::REACH> win;
     win.gather(v);
     uint32_t h[4];
@@ -243,6 +296,29 @@ __device__ __forceinline__ void gauss_strip(const DImg &s, const DImg &d, int bo
       store8(row_ptr<uint8_t>(d, y), gs, n, o8.x, o8.y);
     }
   }
+
+  __device__ __forceinline__ void run() {
+#pragma unroll 1
+    for (int j = 0; j < kQD; j++) {
+      if (j < NR) fetch(j);
+      cp_commit();
+    }
+#pragma unroll
+    for (int a = 0; a < K - 1; a++)
+#pragma unroll
+      for (int i = 0; i < 4; i++) ca[a][i] = 0;
+#pragma unroll 1
+    for (int j = 0; j < NR; j += 2) {
+      step<false>(j);
+      step<true>(j + 1);
+    }
+  }
+};
+
+template <int K, int CN, int RH>
+__device__ __forceinline__ void gauss_strip(const DImg &s, const DImg &d, int border, int tx, int ty, int lane) {
+  GaussStrip<K, CN, RH> g(s, d, border, tx, ty, lane);
+  g.run();
 }
 
 // ---------------------------------------------------------- morphology
@@ -284,10 +360,14 @@ __device__ __forceinline__ void pair_runs(const uint32_t (&own)[4], uint32_t (&r
   }
 }
 
-// Running vertical combination: a[j] collects output row (r - j + ay)
-// while source row r arrives, from element row j.
+// Running vertical combination: logical accumulator j collects the output
+// row that element row j of the current source row contributes to; after
+// each source row the last one is complete and the others move up by one.
+// The accumulators form a ring: at phase PH (source rows added so far, mod
+// KH) logical j lives in slot (j - PH) mod KH, so with the row loop unrolled
+// by KH every slot index is a compile-time constant and nothing moves.
 template <class PR, bool MAX>
-struct Acc {
+struct Ring {
   static constexpr int KH = PR::KH;
   static constexpr uint32_t I = MAX ? 0u : 0x00FF00FFu;
   uint32_t a[KH][4];
@@ -297,24 +377,22 @@ struct Acc {
 #pragma unroll
       for (int p = 0; p < 4; p++) a[j][p] = I;
   }
-  // Adds a row of runs; o receives the completed output row (r - (KH-1) + ay).
-  template <int M>
+  // Adds a row of runs at phase PH; o receives the completed output row.
+  template <int PH, int M>
   __device__ __forceinline__ void add(const uint32_t (&r)[M + 1][4], uint32_t (&o)[4]) {
 #pragma unroll
     for (int j = 0; j < KH; j++) {
+      const int sl = (j + KH - PH) % KH;
       const int dj = PR::at(j);
-      if (dj < 0) continue;
 #pragma unroll
-      for (int p = 0; p < 4; p++) a[j][p] = pop<MAX>(a[j][p], r[dj][p]);
+      for (int p = 0; p < 4; p++) {
+        if (j == 0) a[sl][p] = dj < 0 ? I : r[dj][p];  // a fresh accumulator
+        else if (dj >= 0) a[sl][p] = pop<MAX>(a[sl][p], r[dj][p]);
+      }
     }
+    constexpr int last = (KH - 1 + KH - PH) % KH;
 #pragma unroll
-    for (int p = 0; p < 4; p++) o[p] = a[KH - 1][p];
-#pragma unroll
-    for (int j = KH - 1; j > 0; j--)
-#pragma unroll
-      for (int p = 0; p < 4; p++) a[j][p] = a[j - 1][p];
-#pragma unroll
-    for (int p = 0; p < 4; p++) a[0][p] = I;
+    for (int p = 0; p < 4; p++) o[p] = a[last][p];
   }
 };
 
@@ -332,82 +410,112 @@ __device__ __forceinline__ void mask_pairs(uint32_t (&v)[4], const Cols &c, uint
 }
 
 // One pass (FUSED = false: extremum MAX1 with element P1) or two fused
-// passes (MAX1 with P1, then !MAX1 with P2) over a strip whose outer HALO
-// lanes are not written. A lane's first-pass value at a sample is exact once
-// the samples within its reach exist in the strip, so HALO lanes covering
-// (M1 + M2) * CN samples suffice.
+// passes (MAX1 with P1, then !MAX1 with P2, which has P1's height) over a
+// strip whose outer HALO lanes are not written. A lane's first-pass value at
+// a sample is exact once the samples within its reach exist in the strip, so
+// HALO lanes covering (M1 + M2) * CN samples suffice. Source rows come
+// through the shared-memory row queue; the row loop is unrolled by the
+// element height (ring accumulators).
 template <class P1, class P2, int CN, int RH, bool MAX1, bool FUSED>
 struct MorphStrip {
   static constexpr int M1 = P1::maxd(), M2 = FUSED ? P2::maxd() : 0;
   static constexpr int KH1 = P1::KH, KH2 = FUSED ? P2::KH : 1;
+  static_assert(!FUSED || KH1 == KH2, "fused passes use elements of one height");
   static constexpr int HALO = ((M1 + M2) * CN + kSPL - 1) / kSPL > 0 ? ((M1 + M2) * CN + kSPL - 1) / kSPL : 1;
   static constexpr int OL = 32 - 2 * HALO;
   static constexpr int AY1 = KH1 / 2, AY2 = FUSED ? KH2 / 2 : 0;
   static constexpr int NSRC = RH + (KH1 - 1) + (FUSED ? KH2 - 1 : 0);
+  static constexpr bool MAX2 = !MAX1;
+  static constexpr uint32_t I1 = MAX1 ? 0u : 0xFFFFFFFFu;
+  static constexpr uint32_t I2p = MAX2 ? 0u : 0x00FF00FFu;
 
-  static __device__ __forceinline__ void run(const DImg &s, const DImg &d, int tx, int ty, int lane) {
-    constexpr bool MAX2 = !MAX1;
-    constexpr uint32_t I1 = MAX1 ? 0u : 0xFFFFFFFFu;
-    constexpr uint32_t I2p = MAX2 ? 0u : 0x00FF00FFu;
-    const long long n = (long long)s.w * CN;
-    const long long gs = ((long long)tx * OL - HALO + lane) * kSPL;
-    const Cols c = make_cols<CN, (M1 + M2) * CN>(gs, n, s.w, 0, true, lane);
-    const int H = s.h;
-    const int y0 = ty * RH;
-    const int first = y0 - AY2 - AY1;
-    const bool out_lane = lane >= HALO && lane < 32 - HALO && gs < n;
-    auto load_row = [&](int j) -> uint2 {
-      const int sy = first + j;
-      return (sy < 0 || sy >= H) ? make_uint2(I1, I1) : load8(row_ptr<const uint8_t>(s, sy), c, I1);
-    };
-    Acc<P1, MAX1> acc1;
-    Acc<P2, MAX2> acc2;
-    acc1.init();
-    acc2.init();
-    uint2 q[kPD];
+  const DImg &s, &d;
+  long long n, gs;
+  int H, first;
+  bool out_lane;
+  Cols c;
+  RowQueue q;
+  Ring<P1, MAX1> acc1;
+  Ring<P2, MAX2> acc2;
+
+  __device__ __forceinline__ MorphStrip(const DImg &s_, const DImg &d_, int tx, int ty, int lane) : s(s_), d(d_) {
+    n = (long long)s.w * CN;
+    gs = ((long long)tx * OL - HALO + lane) * kSPL;
+    c = make_cols<CN, (M1 + M2) * CN>(gs, n, s.w, 0, true, lane);
+    H = s.h;
+    first = ty * RH - AY2 - AY1;
+    out_lane = lane >= HALO && lane < 32 - HALO && gs < n;
+    q = row_queue(lane);
+  }
+
+  __device__ __forceinline__ void fetch(int j) {
+    const int sy = first + j;
+    fetch8(q.slot(j), (sy < 0 || sy >= H) ? nullptr : row_ptr<const uint8_t>(s, sy), c, I1);
+  }
+
+  // Source row j; PH = j mod KH1 (the accumulators' phase).
+  template <int PH>
+  __device__ __forceinline__ void step(int j) {
+    if (j >= NSRC) return;
+    cp_wait<kQD - 1>();  // row j has landed
+    const uint2 cur = ld_shared8(q.slot(j));
+    if (j + kQD < NSRC) fetch(j + kQD);
+    cp_commit();
+    uint32_t v[4];
+    unpack_pairs(cur, v);
+    uint32_t r1[M1 + 1][4];
+    pair_runs<M1, CN, MAX1>(v, r1);
+    uint32_t o1[4];
+    acc1.template add<PH, M1>(r1, o1);
+    if (j < KH1 - 1) return;
+    const int y1 = first + j - (KH1 - 1) + AY1;  // first-pass row completed
+    if constexpr (!FUSED) {
+      if (out_lane && y1 < d.h) {
+        const uint2 o8 = pack_pairs(o1);
+        store8(row_ptr<uint8_t>(d, y1), gs, n, o8.x, o8.y);
+      }
+    } else {
+      // First-pass values outside the image are the second pass's identity.
+      if (y1 < 0 || y1 >= H) {
 #pragma unroll
-    for (int k = 0; k < kPD; k++) q[k] = make_uint2(I1, I1);
-    // The first kPD iterations only fill the queue (one load site, rolled).
-#pragma unroll 1
-    for (int j = -kPD; j < NSRC; j++) {
-      const uint2 cur = q[0];
-#pragma unroll
-      for (int k = 0; k < kPD - 1; k++) q[k] = q[k + 1];
-      q[kPD - 1] = j + kPD < NSRC ? load_row(j + kPD) : make_uint2(I1, I1);
-      if (j < 0) continue;
-      uint32_t v[4];
-      unpack_pairs(cur, v);
-      uint32_t r1[M1 + 1][4];
-      pair_runs<M1, CN, MAX1>(v, r1);
-      uint32_t o1[4];
-      acc1.template add<M1>(r1, o1);
-      if (j < KH1 - 1) continue;
-      const int y1 = first + j - (KH1 - 1) + AY1;  // first-pass row completed
-      if constexpr (!FUSED) {
-        if (out_lane && y1 < d.h) {
-          const uint2 o8 = pack_pairs(o1);
-          store8(row_ptr<uint8_t>(d, y1), gs, n, o8.x, o8.y);
-        }
+        for (int p = 0; p < 4; p++) o1[p] = I2p;
       } else {
-        // First-pass values outside the image are the second pass's identity.
-        if (y1 < 0 || y1 >= H) {
-#pragma unroll
-          for (int p = 0; p < 4; p++) o1[p] = I2p;
-        } else {
-          mask_pairs(o1, c, I2p);
-        }
-        uint32_t r2[M2 + 1][4];
-        pair_runs<M2, CN, MAX2>(o1, r2);
-        uint32_t o2[4];
-        acc2.template add<M2>(r2, o2);
-        if (j < (KH1 - 1) + (KH2 - 1)) continue;
-        const int y2 = y1 - (KH2 - 1) + AY2;
-        if (out_lane && y2 < d.h) {
-          const uint2 o8 = pack_pairs(o2);
-          store8(row_ptr<uint8_t>(d, y2), gs, n, o8.x, o8.y);
-        }
+        mask_pairs(o1, c, I2p);
+      }
+      uint32_t r2[M2 + 1][4];
+      pair_runs<M2, CN, MAX2>(o1, r2);
+      uint32_t o2[4];
+      // acc2 has taken j - (KH1 - 1) rows before this one.
+      acc2.template add<(PH + 2 * KH2 - (KH1 - 1) % KH2) % KH2, M2>(r2, o2);
+      if (j < (KH1 - 1) + (KH2 - 1)) return;
+      const int y2 = y1 - (KH2 - 1) + AY2;
+      if (out_lane && y2 < d.h) {
+        const uint2 o8 = pack_pairs(o2);
+        store8(row_ptr<uint8_t>(d, y2), gs, n, o8.x, o8.y);
       }
     }
+  }
+
+  template <int... PH>
+  __device__ __forceinline__ void steps(int j, std::integer_sequence<int, PH...>) {
+    (step<PH>(j + PH), ...);
+  }
+
+  __device__ __forceinline__ void go() {
+    acc1.init();
+    acc2.init();
+#pragma unroll 1
+    for (int j = 0; j < kQD; j++) {
+      if (j < NSRC) fetch(j);
+      cp_commit();
+    }
+#pragma unroll 1
+    for (int j = 0; j < NSRC; j += KH1) steps(j, std::make_integer_sequence<int, KH1>{});
+  }
+
+  static __device__ __forceinline__ void run(const DImg &s, const DImg &d, int tx, int ty, int lane) {
+    MorphStrip m(s, d, tx, ty, lane);
+    m.go();
   }
 };
 
