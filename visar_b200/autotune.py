@@ -5,7 +5,7 @@ launch per shape class. Its tuning table holds, per class key
 `<op>.<depth>.c<channels>.k<ksize>[.<element>][.<pass>].<size class>`
 (the `name` of a launch in `Batch.launch_stats()`), integer fields:
 
-  rows    tile height: rows per tile (strip ops: 8 or 32 rows per warp tile;
+  rows    tile height: rows per tile (strip ops: 8, 32 or 64 rows per warp tile;
           row-tiled ops: rows per thread, the tile being rows x the CTA's
           rows in flight)
   vec     samples (pixels) per thread, i.e. the vector width of the loads
@@ -38,8 +38,8 @@ from . import batch as B
 
 # Candidate values per field, by op (the first word of a class key).
 CANDIDATES = {
-    "gauss_strip": {"rows": (8, 32), "per_sm": (2, 3, 4)},
-    "morph_strip": {"rows": (8, 32), "per_sm": (2, 4, 5, 6)},
+    "gauss_strip": {"rows": (8, 32, 64), "per_sm": (2, 4, 5)},
+    "morph_strip": {"rows": (8, 32, 64), "per_sm": (2, 3, 4)},
     "gauss": {"rows": (8, 16, 32), "per_sm": (2, 4)},
     "morph": {"per_sm": (2, 4)},
     "gray": {"rows": (1, 2, 4, 8, 16), "vec": (8, 16), "per_sm": (2, 4, 6)},

@@ -154,7 +154,7 @@ class Batch:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and lib is not None:  # (module globals are gone at interpreter exit)
             lib.visar_batch_destroy(h)
             self._h = None
 

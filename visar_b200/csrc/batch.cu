@@ -251,12 +251,20 @@ void tune_and_tile(Launch &L, int num_sms) {
       break;
     }
     case kOpGaussStrip: case kOpMorphStrip: {
-      // Warp tiles: 32 rows when there are ~8 per resident warp slot, else 8.
-      L.rows = tuned == 8 || tuned == 32 ? tuned : 32;
-      retile();
-      if (tuned <= 0 && total_tiles(L) < 8LL * num_sms * 16) {
-        L.rows = 8;
+      // Warp tiles of 64 (Gaussian, one-channel morphology), 32 or 8 rows:
+      // the tallest that leaves ~8 tiles per resident warp slot (taller
+      // tiles re-read fewer halo rows).
+      const bool has64 = L.op == kOpGaussStrip || L.cn == 1;
+      if (tuned == 8 || tuned == 32 || (tuned == 64 && has64)) {
+        L.rows = tuned;
         retile();
+        break;
+      }
+      for (const int rh : {64, 32, 8}) {
+        if (rh == 64 && !has64) continue;
+        L.rows = rh;
+        retile();
+        if (total_tiles(L) >= 8LL * num_sms * 24) break;
       }
       break;
     }

@@ -78,7 +78,7 @@ __global__ void __launch_bounds__(Op::kThreads, MinBlocks<Op>::value) k_batch(Ti
     int next = 0;
     if (tid == 0) next = atomicAdd(q.counter, 1);
     const int img = find_image(start, q.n, cur);
-    const BImg &im = q.imgs[img];
+    const BImg im = q.imgs[img];  // a copy: stores through byte pointers cannot alias it
     const int local = cur - start[img];
     const int txn = im.tiles_x;
     Op::tile(im, a, local % txn, local / txn, smem);
@@ -108,7 +108,7 @@ __global__ void __launch_bounds__(Op::kThreads, Op::kMinBlocks) k_batch_warp(Til
   while (cur < q.total) {
     if (lane == 0) t = atomicAdd(q.counter, 1);
     const int img = find_image(start, q.n, cur);
-    const BImg &im = q.imgs[img];
+    const BImg im = q.imgs[img];  // a copy: stores through byte pointers cannot alias it
     const int local = cur - start[img];
     const int txn = im.tiles_x;
     Op::tile(im, a, local % txn, local / txn, lane);
@@ -238,7 +238,7 @@ __device__ __forceinline__ uint32_t gray_px(uint32_t b, uint32_t g, uint32_t r) 
 // thread.
 template <int SCN, int P>
 struct OpGray {
-  static constexpr int kThreads = 256;
+  static constexpr int kThreads = 256, kMinBlocks = P == 16 ? 4 : 5;  // <= 64 / 48 registers
   using Args = RowArgs;
   static size_t smem(const Args &) { return 0; }
   static __device__ __forceinline__ void px(const Vb<P, SCN> &in, Vb<P, 1> &out) {
@@ -287,7 +287,7 @@ struct OpGray {
 // Exact halving (resize_u8.zig:381-447), P = 4 or 8 output pixels per thread.
 template <int CN, int P>
 struct OpHalf {
-  static constexpr int kThreads = 256;
+  static constexpr int kThreads = 256, kMinBlocks = P * CN >= 24 ? 3 : P * CN > 8 ? 4 : 5;  // <= 80 / 64 / 48 registers
   using Args = RowArgs;
   static size_t smem(const Args &) { return 0; }
   // Output samples of one output row from its two source rows.
@@ -350,7 +350,7 @@ struct OpHalf {
 // pixel per thread, two output rows (four source rows) in flight.
 template <int CN>
 struct OpLinear {
-  static constexpr int kThreads = 256;
+  static constexpr int kThreads = 256, kMinBlocks = CN == 1 ? 5 : CN == 4 ? 3 : 4;  // <= 48 / 64 / 80 registers
   using Args = RowArgs;
   static size_t smem(const Args &) { return 0; }
   static __device__ __forceinline__ void tile(const BImg &im, const Args &a, int tx, int ty, unsigned char *) {
@@ -406,7 +406,7 @@ struct LutArgs {
 // samples per thread.
 template <int P>
 struct OpLut {
-  static constexpr int kThreads = 256;
+  static constexpr int kThreads = 256, kMinBlocks = 5;  // <= 48 registers
   using Args = LutArgs;
   static size_t smem(const Args &) { return 256; }
   static __device__ __forceinline__ void tile(const BImg &im, const Args &a, int tx, int ty, unsigned char *smem) {
@@ -471,7 +471,7 @@ struct NoArgs {
 // on warp strips (strip.cuh).
 template <class P1, class P2, int CN, int RH, bool MAX1, bool FUSED>
 struct OpMorphStrip {
-  static constexpr int kThreads = 128, kMinBlocks = FUSED ? 5 : 6;  // 102 / 85 registers
+  static constexpr int kThreads = 128, kMinBlocks = FUSED ? (P1::KH >= 7 ? 4 : 5) : 6;  // 128 / 102 / 85 registers
   static constexpr bool kWarpTiles = true;
   using Args = NoArgs;
   static size_t smem(const Args &) { return 0; }
@@ -588,8 +588,11 @@ cudaError_t launch_morph_strip_rh(const LaunchRun &r, bool max1, bool fused, cud
 
 template <class PR, int CN>
 cudaError_t launch_morph_strip_prof(const LaunchRun &r, int rows, bool max1, bool fused, cudaStream_t st) {
-  return rows == 8 ? launch_morph_strip_rh<PR, CN, 8>(r, max1, fused, st)
-                   : launch_morph_strip_rh<PR, CN, 32>(r, max1, fused, st);
+  if (rows == 8) return launch_morph_strip_rh<PR, CN, 8>(r, max1, fused, st);
+  if constexpr (CN == 1) {  // 64-row tiles: one-channel images only (compile time)
+    if (rows == 64) return launch_morph_strip_rh<PR, CN, 64>(r, max1, fused, st);
+  }
+  return launch_morph_strip_rh<PR, CN, 32>(r, max1, fused, st);
 }
 
 template <int CN>

@@ -209,6 +209,18 @@ __device__ __forceinline__ void fetch8(uint32_t saddr, const uint8_t *row, const
   else st_shared8(saddr, make_uint2(fill, fill));
 }
 
+// Interior tiles (every lane's samples inside the row): a predicated copy of
+// the lane's 8 samples at g, or the fill stored into the slot when !p (g is
+// then not read). No branches.
+__device__ __forceinline__ void fetch8_inside(uint32_t saddr, const uint8_t *g, bool p, uint32_t fill) {
+  asm volatile(
+      "{\n .reg .pred q;\n setp.ne.b32 q, %2, 0;\n"
+      " @q cp.async.ca.shared.global [%0], [%1], 8;\n"
+      " @!q st.shared.v2.u32 [%0], {%3, %3};\n}\n" ::"r"(saddr),
+      "l"(g), "r"((int)p), "r"(fill)
+      : "memory");
+}
+
 // One strip tile: lanes cover samples [(tx*OL - HALO + lane) * 8, +8) of
 // rows [ty*RH, ty*RH + RH). The vertical binomial runs as a cascade of
 // pairwise sums over the incoming rows (its state alternates between two
@@ -222,14 +234,14 @@ struct GaussStrip {
   static constexpr int E = Binom<K>::e;
   static constexpr int SH = 16 - 2 * E;
   static constexpr uint32_t RND = (1u << (SH - 1)) * 0x00010001u;
-  static_assert(NR % 2 == 0, "rows per tile plus the stencil's halo must be even");
 
-  const DImg &s, &d;
-  int border, y0;
+  const DImg s, d;  // copies (kept in registers across the row loop)
+  int border, y0, nr;
   long long n, gs;
   bool out_lane;
   Cols c;
   RowQueue q;
+  int lo[R], hi[R];  // border-mapped rows -R..-1 and h..h+R-1 (-1: constant fill)
   uint32_t ca[K - 1][4], cb[K - 1][4];
 
   __device__ __forceinline__ GaussStrip(const DImg &s_, const DImg &d_, int border_, int tx, int ty, int lane)
@@ -239,28 +251,46 @@ struct GaussStrip {
     c = make_cols<CN, G::REACH>(gs, n, s.w, border, false, lane);
     out_lane = lane >= HALO && lane < 32 - HALO && gs < n;
     q = row_queue(lane);
-  }
-
-  // Source row j of the tile (image row y0 - R + j, border-mapped) into its slot.
-  __device__ __forceinline__ void fetch(int j) {
-    const int sy = y0 - R + j;
-    const uint8_t *row = nullptr;
-    if (sy >= 0 && sy < s.h) {
-      row = row_ptr<const uint8_t>(s, sy);
-    } else {
-      const int my = border_map(sy, s.h, border);
-      if (my >= 0) row = row_ptr<const uint8_t>(s, my);
+    // Only the rows the tile's outputs (y < h) need: at most R past the image.
+    nr = min(NR, d.h - y0 + K - 1);
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      lo[r] = border_map(r - R, s.h, border);
+      hi[r] = border_map(s.h + r, s.h, border);
     }
-    fetch8(q.slot(j), row, c, 0u);
   }
 
-  template <bool ODD>
+  // Image row of source row j (y0 - R + j, border-mapped; -1: constant fill).
+  __device__ __forceinline__ int map_row(int j) const {
+    const int sy = y0 - R + j;
+    int my = sy;
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      my = sy == r - R ? lo[r] : my;
+      my = sy == s.h + r ? hi[r] : my;
+    }
+    return my;
+  }
+
+  // Source row j into its slot.
+  template <bool INSIDE>
+  __device__ __forceinline__ void fetch(int j) {
+    const int my = map_row(j);
+    if constexpr (INSIDE) {
+      const uint8_t *row = row_ptr<const uint8_t>(s, my < 0 ? 0 : my);
+      fetch8_inside(q.slot(j), row + gs, my >= 0, 0u);
+    } else {
+      fetch8(q.slot(j), my < 0 ? nullptr : row_ptr<const uint8_t>(s, my), c, 0u);
+    }
+  }
+
+  template <bool INSIDE, bool ODD>
   __device__ __forceinline__ void step(int j) {
     const uint32_t(&in)[K - 1][4] = ODD ? cb : ca;
     uint32_t(&out)[K - 1][4] = ODD ? ca : cb;
     cp_wait<kQD - 1>();  // row j has landed
     const uint2 cur = ld_shared8(q.slot(j));
-    if (j + kQD < NR) fetch(j + kQD);
+    if (j + kQD < nr) fetch<INSIDE>(j + kQD);
     cp_commit();
     // Cascade of pairwise sums: after row j the last stage holds the
     // binomial sum of rows j-K+1..j.
@@ -282,25 +312,30 @@ struct GaussStrip {
     for (int o = 0; o < 4; o++) {
       const int c0 = 2 * o;
       if constexpr (K == 3) {
-        h[o] = win.at(c0 - CN) + win.at(c0 + CN) + (win.at(c0) << 1);
+        h[o] = win.at(c0 - CN) + win.at(c0 + CN) + (win.at(c0) << 1) + RND;
       } else {
-        const uint32_t a = win.at(c0 - 2 * CN) + win.at(c0 + 2 * CN);
-        const uint32_t b = win.at(c0 - CN) + win.at(c0 + CN);
-        h[o] = a + (b << 2) + win.at(c0) * 6u;
+        // a + 4 b + 6 x = (l2 + r2) + 4 (l1 + r1 + x) + 2 x
+        const uint32_t x = win.at(c0);
+        const uint32_t a = win.at(c0 - 2 * CN) + win.at(c0 + 2 * CN) + RND;
+        const uint32_t b = win.at(c0 - CN) + win.at(c0 + CN) + x;
+        h[o] = a + (b << 2) + (x << 1);
       }
-      h[o] = (h[o] + RND) >> SH;
+      h[o] >>= SH;
     }
-    const int y = y0 + j - (K - 1);
-    if (out_lane && y < d.h) {
-      const uint2 o8 = pack_pairs(h);
-      store8(row_ptr<uint8_t>(d, y), gs, n, o8.x, o8.y);
+    const int y = y0 + j - (K - 1);  // < d.h: rows are trimmed to the image
+    const uint2 o8 = pack_pairs(h);
+    if constexpr (INSIDE) {
+      if (out_lane) *reinterpret_cast<uint2 *>(row_ptr<uint8_t>(d, y) + gs) = o8;
+    } else {
+      if (out_lane) store8(row_ptr<uint8_t>(d, y), gs, n, o8.x, o8.y);
     }
   }
 
-  __device__ __forceinline__ void run() {
+  template <bool INSIDE>
+  __device__ __forceinline__ void rows() {
 #pragma unroll 1
     for (int j = 0; j < kQD; j++) {
-      if (j < NR) fetch(j);
+      if (j < nr) fetch<INSIDE>(j);
       cp_commit();
     }
 #pragma unroll
@@ -308,10 +343,15 @@ struct GaussStrip {
 #pragma unroll
       for (int i = 0; i < 4; i++) ca[a][i] = 0;
 #pragma unroll 1
-    for (int j = 0; j < NR; j += 2) {
-      step<false>(j);
-      step<true>(j + 1);
+    for (int j = 0; j < nr; j += 2) {
+      step<INSIDE, false>(j);
+      if (j + 1 < nr) step<INSIDE, true>(j + 1);
     }
+  }
+
+  __device__ __forceinline__ void run() {
+    if (__all_sync(kFull, c.inside)) rows<true>();
+    else rows<false>();
   }
 };
 
@@ -429,9 +469,9 @@ struct MorphStrip {
   static constexpr uint32_t I1 = MAX1 ? 0u : 0xFFFFFFFFu;
   static constexpr uint32_t I2p = MAX2 ? 0u : 0x00FF00FFu;
 
-  const DImg &s, &d;
+  const DImg s, d;  // copies (kept in registers across the row loop)
   long long n, gs;
-  int H, first;
+  int H, first, nsrc;
   bool out_lane;
   Cols c;
   RowQueue q;
@@ -443,23 +483,42 @@ struct MorphStrip {
     gs = ((long long)tx * OL - HALO + lane) * kSPL;
     c = make_cols<CN, (M1 + M2) * CN>(gs, n, s.w, 0, true, lane);
     H = s.h;
-    first = ty * RH - AY2 - AY1;
+    const int y0 = ty * RH;
+    first = y0 - AY2 - AY1;
+    // Only the source rows the tile's outputs (y < h) need.
+    nsrc = min(NSRC, min(y0 + RH, d.h) - y0 + KH1 + KH2 - 2);
     out_lane = lane >= HALO && lane < 32 - HALO && gs < n;
     q = row_queue(lane);
   }
 
+  template <bool INSIDE>
   __device__ __forceinline__ void fetch(int j) {
     const int sy = first + j;
-    fetch8(q.slot(j), (sy < 0 || sy >= H) ? nullptr : row_ptr<const uint8_t>(s, sy), c, I1);
+    const bool in = sy >= 0 && sy < H;
+    if constexpr (INSIDE) {
+      fetch8_inside(q.slot(j), row_ptr<const uint8_t>(s, in ? sy : 0) + gs, in, I1);
+    } else {
+      fetch8(q.slot(j), in ? row_ptr<const uint8_t>(s, sy) : nullptr, c, I1);
+    }
+  }
+
+  template <bool INSIDE>
+  __device__ __forceinline__ void put(int y, const uint32_t (&o)[4]) {
+    const uint2 o8 = pack_pairs(o);
+    if constexpr (INSIDE) {
+      if (out_lane) *reinterpret_cast<uint2 *>(row_ptr<uint8_t>(d, y) + gs) = o8;
+    } else {
+      if (out_lane) store8(row_ptr<uint8_t>(d, y), gs, n, o8.x, o8.y);
+    }
   }
 
   // Source row j; PH = j mod KH1 (the accumulators' phase).
-  template <int PH>
+  template <bool INSIDE, int PH>
   __device__ __forceinline__ void step(int j) {
-    if (j >= NSRC) return;
+    if (j >= nsrc) return;
     cp_wait<kQD - 1>();  // row j has landed
     const uint2 cur = ld_shared8(q.slot(j));
-    if (j + kQD < NSRC) fetch(j + kQD);
+    if (j + kQD < nsrc) fetch<INSIDE>(j + kQD);
     cp_commit();
     uint32_t v[4];
     unpack_pairs(cur, v);
@@ -468,18 +527,15 @@ struct MorphStrip {
     uint32_t o1[4];
     acc1.template add<PH, M1>(r1, o1);
     if (j < KH1 - 1) return;
-    const int y1 = first + j - (KH1 - 1) + AY1;  // first-pass row completed
+    const int y1 = first + j - (KH1 - 1) + AY1;  // first-pass row completed (< d.h when !FUSED)
     if constexpr (!FUSED) {
-      if (out_lane && y1 < d.h) {
-        const uint2 o8 = pack_pairs(o1);
-        store8(row_ptr<uint8_t>(d, y1), gs, n, o8.x, o8.y);
-      }
+      put<INSIDE>(y1, o1);
     } else {
       // First-pass values outside the image are the second pass's identity.
       if (y1 < 0 || y1 >= H) {
 #pragma unroll
         for (int p = 0; p < 4; p++) o1[p] = I2p;
-      } else {
+      } else if constexpr (!INSIDE) {
         mask_pairs(o1, c, I2p);
       }
       uint32_t r2[M2 + 1][4];
@@ -488,34 +544,32 @@ struct MorphStrip {
       // acc2 has taken j - (KH1 - 1) rows before this one.
       acc2.template add<(PH + 2 * KH2 - (KH1 - 1) % KH2) % KH2, M2>(r2, o2);
       if (j < (KH1 - 1) + (KH2 - 1)) return;
-      const int y2 = y1 - (KH2 - 1) + AY2;
-      if (out_lane && y2 < d.h) {
-        const uint2 o8 = pack_pairs(o2);
-        store8(row_ptr<uint8_t>(d, y2), gs, n, o8.x, o8.y);
-      }
+      put<INSIDE>(y1 - (KH2 - 1) + AY2, o2);  // < d.h: rows are trimmed to the image
     }
   }
 
-  template <int... PH>
+  template <bool INSIDE, int... PH>
   __device__ __forceinline__ void steps(int j, std::integer_sequence<int, PH...>) {
-    (step<PH>(j + PH), ...);
+    (step<INSIDE, PH>(j + PH), ...);
   }
 
-  __device__ __forceinline__ void go() {
+  template <bool INSIDE>
+  __device__ __forceinline__ void rows() {
     acc1.init();
     acc2.init();
 #pragma unroll 1
     for (int j = 0; j < kQD; j++) {
-      if (j < NSRC) fetch(j);
+      if (j < nsrc) fetch<INSIDE>(j);
       cp_commit();
     }
 #pragma unroll 1
-    for (int j = 0; j < NSRC; j += KH1) steps(j, std::make_integer_sequence<int, KH1>{});
+    for (int j = 0; j < nsrc; j += KH1) steps<INSIDE>(j, std::make_integer_sequence<int, KH1>{});
   }
 
   static __device__ __forceinline__ void run(const DImg &s, const DImg &d, int tx, int ty, int lane) {
     MorphStrip m(s, d, tx, ty, lane);
-    m.go();
+    if (__all_sync(kFull, m.c.inside)) m.template rows<true>();
+    else m.template rows<false>();
   }
 };
 

@@ -72,7 +72,7 @@ class Server:
         self._keep = {}
 
     def close(self):
-        if getattr(self, "_h", None):
+        if getattr(self, "_h", None) and lib is not None:  # (module globals are gone at interpreter exit)
             lib.visar_server_destroy(self._h)
             self._h = None
 
