@@ -175,19 +175,19 @@ struct GaussGeom {
 constexpr int kQD = 8;
 
 __device__ __forceinline__ void cp_async8(uint32_t saddr, const void *g) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(saddr), "l"(g) : "memory");
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(saddr), "l"(g));
 }
-__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n"); }
 template <int N>
 __device__ __forceinline__ void cp_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 __device__ __forceinline__ void st_shared8(uint32_t saddr, uint2 v) {
-  asm volatile("st.shared.v2.u32 [%0], {%1, %2};\n" ::"r"(saddr), "r"(v.x), "r"(v.y) : "memory");
+  asm volatile("st.shared.v2.u32 [%0], {%1, %2};\n" ::"r"(saddr), "r"(v.x), "r"(v.y));
 }
 __device__ __forceinline__ uint2 ld_shared8(uint32_t saddr) {
   uint2 v;
-  asm volatile("ld.shared.v2.u32 {%0, %1}, [%2];\n" : "=r"(v.x), "=r"(v.y) : "r"(saddr) : "memory");
+  asm volatile("ld.shared.v2.u32 {%0, %1}, [%2];\n" : "=r"(v.x), "=r"(v.y) : "r"(saddr));
   return v;
 }
 
@@ -217,8 +217,15 @@ __device__ __forceinline__ void fetch8_inside(uint32_t saddr, const uint8_t *g, 
       "{\n .reg .pred q;\n setp.ne.b32 q, %2, 0;\n"
       " @q cp.async.ca.shared.global [%0], [%1], 8;\n"
       " @!q st.shared.v2.u32 [%0], {%3, %3};\n}\n" ::"r"(saddr),
-      "l"(g), "r"((int)p), "r"(fill)
-      : "memory");
+      "l"(g), "r"((int)p), "r"(fill));
+}
+
+// 8 bytes to global memory when p (no branch).
+__device__ __forceinline__ void st_global8_if(uint8_t *g, uint2 v, bool p) {
+  asm volatile(
+      "{\n .reg .pred q;\n setp.ne.b32 q, %3, 0;\n"
+      " @q st.global.v2.u32 [%0], {%1, %2};\n}\n" ::"l"(g),
+      "r"(v.x), "r"(v.y), "r"((int)p));
 }
 
 // One strip tile: lanes cover samples [(tx*OL - HALO + lane) * 8, +8) of
@@ -272,25 +279,27 @@ struct GaussStrip {
     return my;
   }
 
-  // Source row j into its slot.
+  // Source row j into its slot (rows j >= nr: nothing is read).
   template <bool INSIDE>
   __device__ __forceinline__ void fetch(int j) {
     const int my = map_row(j);
     if constexpr (INSIDE) {
       const uint8_t *row = row_ptr<const uint8_t>(s, my < 0 ? 0 : my);
-      fetch8_inside(q.slot(j), row + gs, my >= 0, 0u);
+      fetch8_inside(q.slot(j), row + gs, my >= 0 && j < nr, 0u);
     } else {
-      fetch8(q.slot(j), my < 0 ? nullptr : row_ptr<const uint8_t>(s, my), c, 0u);
+      if (j < nr) fetch8(q.slot(j), my < 0 ? nullptr : row_ptr<const uint8_t>(s, my), c, 0u);
     }
   }
 
-  template <bool INSIDE, bool ODD>
+  // Source row j. OUT: the cascade is full (j >= K - 1) and row j - (K - 1)
+  // is written when it lies in the image.
+  template <bool INSIDE, bool ODD, bool OUT>
   __device__ __forceinline__ void step(int j) {
     const uint32_t(&in)[K - 1][4] = ODD ? cb : ca;
     uint32_t(&out)[K - 1][4] = ODD ? ca : cb;
     cp_wait<kQD - 1>();  // row j has landed
     const uint2 cur = ld_shared8(q.slot(j));
-    if (j + kQD < nr) fetch<INSIDE>(j + kQD);
+    fetch<INSIDE>(j + kQD);
     cp_commit();
     // Cascade of pairwise sums: after row j the last stage holds the
     // binomial sum of rows j-K+1..j.
@@ -304,7 +313,7 @@ struct GaussStrip {
         out[a][i] = v[i];
         v[i] = t;
       }
-    if (j < K - 1) return;  // window not full yet (warp-uniform)
+    if constexpr (!OUT) return;
     Window<HALO, -G::REACH, kSPL - 1 + G::REACH> win;
     win.gather(v);
     uint32_t h[4];
@@ -322,20 +331,22 @@ struct GaussStrip {
       }
       h[o] >>= SH;
     }
-    const int y = y0 + j - (K - 1);  // < d.h: rows are trimmed to the image
+    const int y = y0 + j - (K - 1);
+    const bool ok = out_lane && y < d.h;
     const uint2 o8 = pack_pairs(h);
     if constexpr (INSIDE) {
-      if (out_lane) *reinterpret_cast<uint2 *>(row_ptr<uint8_t>(d, y) + gs) = o8;
+      st_global8_if(row_ptr<uint8_t>(d, ok ? y : 0) + gs, o8, ok);
     } else {
-      if (out_lane) store8(row_ptr<uint8_t>(d, y), gs, n, o8.x, o8.y);
+      if (ok) store8(row_ptr<uint8_t>(d, y), gs, n, o8.x, o8.y);
     }
   }
 
   template <bool INSIDE>
   __device__ __forceinline__ void rows() {
+    static_assert((K - 1) % 2 == 0, "the cascade fills in pairs of rows");
 #pragma unroll 1
     for (int j = 0; j < kQD; j++) {
-      if (j < nr) fetch<INSIDE>(j);
+      fetch<INSIDE>(j);
       cp_commit();
     }
 #pragma unroll
@@ -343,9 +354,15 @@ struct GaussStrip {
 #pragma unroll
       for (int i = 0; i < 4; i++) ca[a][i] = 0;
 #pragma unroll 1
-    for (int j = 0; j < nr; j += 2) {
-      step<INSIDE, false>(j);
-      if (j + 1 < nr) step<INSIDE, true>(j + 1);
+    for (int j = 0; j < K - 1; j += 2) {
+      step<INSIDE, false, false>(j);
+      step<INSIDE, true, false>(j + 1);
+    }
+    // Pairs of rows; an odd nr ends with one row past the image (not stored).
+#pragma unroll 1
+    for (int j = K - 1; j < nr; j += 2) {
+      step<INSIDE, false, true>(j);
+      step<INSIDE, true, true>(j + 1);
     }
   }
 
@@ -471,7 +488,7 @@ struct MorphStrip {
 
   const DImg s, d;  // copies (kept in registers across the row loop)
   long long n, gs;
-  int H, first, nsrc;
+  int H, first, nsrc, ylim;
   bool out_lane;
   Cols c;
   RowQueue q;
@@ -486,39 +503,43 @@ struct MorphStrip {
     const int y0 = ty * RH;
     first = y0 - AY2 - AY1;
     // Only the source rows the tile's outputs (y < h) need.
-    nsrc = min(NSRC, min(y0 + RH, d.h) - y0 + KH1 + KH2 - 2);
+    ylim = min(y0 + RH, d.h);
+    nsrc = min(NSRC, ylim - y0 + KH1 + KH2 - 2);
     out_lane = lane >= HALO && lane < 32 - HALO && gs < n;
     q = row_queue(lane);
   }
 
+  // Source row j into its slot (rows j >= nsrc: nothing is read).
   template <bool INSIDE>
   __device__ __forceinline__ void fetch(int j) {
     const int sy = first + j;
     const bool in = sy >= 0 && sy < H;
     if constexpr (INSIDE) {
-      fetch8_inside(q.slot(j), row_ptr<const uint8_t>(s, in ? sy : 0) + gs, in, I1);
+      fetch8_inside(q.slot(j), row_ptr<const uint8_t>(s, in ? sy : 0) + gs, in && j < nsrc, I1);
     } else {
-      fetch8(q.slot(j), in ? row_ptr<const uint8_t>(s, sy) : nullptr, c, I1);
+      if (j < nsrc) fetch8(q.slot(j), in ? row_ptr<const uint8_t>(s, sy) : nullptr, c, I1);
     }
   }
 
+  // Output row y, written when it belongs to the tile and the image.
   template <bool INSIDE>
   __device__ __forceinline__ void put(int y, const uint32_t (&o)[4]) {
     const uint2 o8 = pack_pairs(o);
+    const bool ok = out_lane && y < ylim;
     if constexpr (INSIDE) {
-      if (out_lane) *reinterpret_cast<uint2 *>(row_ptr<uint8_t>(d, y) + gs) = o8;
+      st_global8_if(row_ptr<uint8_t>(d, ok ? y : 0) + gs, o8, ok);
     } else {
-      if (out_lane) store8(row_ptr<uint8_t>(d, y), gs, n, o8.x, o8.y);
+      if (ok) store8(row_ptr<uint8_t>(d, y), gs, n, o8.x, o8.y);
     }
   }
 
-  // Source row j; PH = j mod KH1 (the accumulators' phase).
+  // Source row j; PH = j mod KH1 (the accumulators' phase). Rows past nsrc
+  // (the last group of KH1) compute values that are not stored.
   template <bool INSIDE, int PH>
   __device__ __forceinline__ void step(int j) {
-    if (j >= nsrc) return;
     cp_wait<kQD - 1>();  // row j has landed
     const uint2 cur = ld_shared8(q.slot(j));
-    if (j + kQD < nsrc) fetch<INSIDE>(j + kQD);
+    fetch<INSIDE>(j + kQD);
     cp_commit();
     uint32_t v[4];
     unpack_pairs(cur, v);
@@ -527,24 +548,22 @@ struct MorphStrip {
     uint32_t o1[4];
     acc1.template add<PH, M1>(r1, o1);
     if (j < KH1 - 1) return;
-    const int y1 = first + j - (KH1 - 1) + AY1;  // first-pass row completed (< d.h when !FUSED)
+    const int y1 = first + j - (KH1 - 1) + AY1;  // first-pass row completed
     if constexpr (!FUSED) {
       put<INSIDE>(y1, o1);
     } else {
       // First-pass values outside the image are the second pass's identity.
-      if (y1 < 0 || y1 >= H) {
+      const bool rin = y1 >= 0 && y1 < H;
 #pragma unroll
-        for (int p = 0; p < 4; p++) o1[p] = I2p;
-      } else if constexpr (!INSIDE) {
-        mask_pairs(o1, c, I2p);
-      }
+      for (int p = 0; p < 4; p++) o1[p] = rin ? o1[p] : I2p;
+      if constexpr (!INSIDE) mask_pairs(o1, c, I2p);
       uint32_t r2[M2 + 1][4];
       pair_runs<M2, CN, MAX2>(o1, r2);
       uint32_t o2[4];
       // acc2 has taken j - (KH1 - 1) rows before this one.
       acc2.template add<(PH + 2 * KH2 - (KH1 - 1) % KH2) % KH2, M2>(r2, o2);
       if (j < (KH1 - 1) + (KH2 - 1)) return;
-      put<INSIDE>(y1 - (KH2 - 1) + AY2, o2);  // < d.h: rows are trimmed to the image
+      put<INSIDE>(y1 - (KH2 - 1) + AY2, o2);
     }
   }
 
@@ -559,7 +578,7 @@ struct MorphStrip {
     acc2.init();
 #pragma unroll 1
     for (int j = 0; j < kQD; j++) {
-      if (j < nsrc) fetch<INSIDE>(j);
+      fetch<INSIDE>(j);
       cp_commit();
     }
 #pragma unroll 1
