@@ -45,7 +45,7 @@ CANDIDATES = {
     "gray": {"rows": (1, 2, 4, 8, 16), "vec": (8, 16), "per_sm": (2, 4, 6)},
     "lut": {"rows": (1, 2, 4, 8, 16), "vec": (8, 16), "per_sm": (2, 4, 6)},
     "half": {"rows": (1, 2, 4, 8, 16), "vec": (4, 8), "per_sm": (2, 4, 6)},
-    "linear": {"rows": (1, 2, 4, 8, 16), "per_sm": (2, 4, 6)},
+    "linear": {"rows": (2, 4, 8, 16, 32), "per_sm": (2, 4, 6)},
     "warp_affine": {"per_sm": (2, 4, 8)},
     "warp_perspective": {"per_sm": (2, 4, 8)},
 }

@@ -189,7 +189,14 @@ void set_tiles(const Launch &L, BImg &b) {
       break;
     case kOpGray: row_tiles(b, b.s.w, L.vec, L.rows, b.s.h); break;
     case kOpHalf: row_tiles(b, b.d.w, L.vec, L.rows, b.d.h); break;
-    case kOpLinear: row_tiles(b, b.d.w, 1, L.rows, b.d.h); break;
+    case kOpLinear:
+      if (L.cn == 1) {  // OpLinearStrip warp tiles
+        b.tiles_x = (int)ceil_div(b.d.w, OpLinearStrip::kTW);
+        b.tiles_y = (int)ceil_div(b.d.h, L.rows);
+      } else {
+        row_tiles(b, b.d.w, 1, L.rows, b.d.h);
+      }
+      break;
     case kOpLut: row_tiles(b, (long long)b.s.w * b.s.cn, L.vec, L.rows, b.s.h); break;
     case kOpGaussStrip: {
       const int halo = ((L.k / 2) * L.cn + strip::kSPL - 1) / strip::kSPL;
@@ -234,7 +241,24 @@ void tune_and_tile(Launch &L, int num_sms) {
       L.rows = tuned == 8 || tuned == 16 || tuned == 32 ? tuned : 16;
       retile();
       break;
-    case kOpGray: case kOpHalf: case kOpLinear: case kOpLut: {
+    case kOpLinear:
+      if (L.cn == 1) {
+        // Warp tiles: the tallest of 32..4 rows leaving ~8 tiles per warp slot.
+        L.vec = 1;
+        if (tuned > 0) {
+          L.rows = std::min(tuned, 64);
+          retile();
+          break;
+        }
+        for (const int rh : {32, 16, 8, 4}) {
+          L.rows = rh;
+          retile();
+          if (total_tiles(L) >= 8LL * num_sms * 24) break;
+        }
+        break;
+      }
+      [[fallthrough]];
+    case kOpGray: case kOpHalf: case kOpLut: {
       // Samples per thread (vector width): 8 or 16 bytes for gray and the
       // LUT, 4 or 8 output pixels for the halving.
       const int vec = get("vec", -1);
@@ -715,7 +739,7 @@ cudaError_t run_launch(const Plan &P, const Launch &L, cudaStream_t st) {
       return run_half<4>(P, L, ra, st);
     case kOpLinear:
       switch (L.cn) {
-        case 1: return run_op<OpLinear<1>>(P, L, ra, st);
+        case 1: return run_op<OpLinearStrip>(P, L, ra, st);
         case 2: return run_op<OpLinear<2>>(P, L, ra, st);
         case 3: return run_op<OpLinear<3>>(P, L, ra, st);
         default: return run_op<OpLinear<4>>(P, L, ra, st);

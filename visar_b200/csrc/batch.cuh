@@ -397,6 +397,107 @@ struct OpLinear {
   }
 };
 
+// The same bilinear for one-channel images on warp tiles of 128 output
+// pixels (4 per lane) x `rows` rows. For each output row the two source rows'
+// byte spans the tile needs are copied to shared memory with 16-byte cp.async
+// (coalesced, kRing - 1 rows ahead), and the lanes read their taps from
+// there. Tiles whose span exceeds kSpan bytes (shrinking by more than ~3.9x),
+// or sources whose rows are not 16-byte aligned, read their taps directly.
+struct OpLinearStrip {
+  static constexpr int kThreads = 128, kMinBlocks = 6;
+  static constexpr bool kWarpTiles = true;
+  static constexpr int kPX = 4, kTW = 32 * kPX, kSpan = 512, kRing = 4;
+  using Args = RowArgs;
+  static size_t smem(const Args &) { return 0; }
+
+  static __device__ __forceinline__ uint32_t px(uint32_t a, uint32_t b, uint32_t c, uint32_t e, const int4 &t,
+                                                int w0, int w1) {
+    const int h0 = ((int)a * t.z + (int)b * t.w) >> 4;
+    const int h1 = ((int)c * t.z + (int)e * t.w) >> 4;
+    const int v = ((h0 * w0) >> 16) + ((h1 * w1) >> 16);
+    return (uint32_t)min(max((v + 2) >> 2, 0), 255);
+  }
+
+  static __device__ __forceinline__ void put(const DImg &d, int y, int x, int dw, uint32_t out) {
+    uint8_t *o = row_ptr<uint8_t>(d, y) + x;
+    if (x + kPX <= dw && ((uintptr_t)o & 3) == 0) {
+      *reinterpret_cast<uint32_t *>(o) = out;
+    } else {
+      for (int k = 0; k < kPX && x + k < dw; k++) o[k] = (uint8_t)(out >> (8 * k));
+    }
+  }
+
+  static __device__ __forceinline__ void tile(const BImg &im, const Args &a, int tx, int ty, int lane) {
+    __shared__ __align__(16) uint8_t s_buf[4][kRing][2][kSpan];
+    const DImg s = im.s, d = im.d;
+    const int dw = d.w;
+    const int x = tx * kTW + lane * kPX;
+    const int ybeg = ty * a.rows, yend = min(d.h, ybeg + a.rows);
+    const int4 *xt = static_cast<const int4 *>(im.t0);
+    const LinTap *yt = static_cast<const LinTap *>(im.t1);
+    int4 t[kPX];
+#pragma unroll
+    for (int k = 0; k < kPX; k++) t[k] = xt[min(x + k, dw - 1)];
+    // The tile's source span [lo, hi] (x taps are monotonic; pixels past dw
+    // repeat the last one).
+    const int lo = (int)__reduce_min_sync(strip::kFull, (unsigned)t[0].x);
+    const int hi = (int)__reduce_max_sync(strip::kFull, (unsigned)t[kPX - 1].y);
+    const int a0 = lo & ~15;
+    const int nb = hi + 1 - a0;
+    const bool staged = nb <= kSpan && (((uintptr_t)s.p | (uintptr_t)s.stride) & 15) == 0;
+    if (!staged) {
+      for (int y = ybeg; y < yend; y++) {
+        const LinTap r = yt[y];
+        const uint8_t *q0 = row_ptr<const uint8_t>(s, r.o0), *q1 = row_ptr<const uint8_t>(s, r.o1);
+        uint32_t out = 0;
+#pragma unroll
+        for (int k = 0; k < kPX; k++)
+          out |= px(__ldg(q0 + t[k].x), __ldg(q0 + t[k].y), __ldg(q1 + t[k].x), __ldg(q1 + t[k].y), t[k], r.w0, r.w1)
+                 << (8 * k);
+        if (x < dw) put(d, y, x, dw, out);
+      }
+      return;
+    }
+    const int nch = (nb + 15) >> 4;  // 16-byte chunks per source row (<= 32)
+    uint8_t(*buf)[2][kSpan] = s_buf[(threadIdx.x >> 5) & 3];
+    // Copies of output row y's two source spans into ring slot y % kRing
+    // (an empty group past the tile, so every row waits the same way).
+    auto issue = [&](int y) {
+      if (y < yend && lane < nch) {
+        const LinTap r = yt[y];
+        const uint32_t d0 = (uint32_t)__cvta_generic_to_shared(&buf[y % kRing][0][lane * 16]);
+        const uint32_t d1 = (uint32_t)__cvta_generic_to_shared(&buf[y % kRing][1][lane * 16]);
+        const uint8_t *g0 = row_ptr<const uint8_t>(s, r.o0) + a0 + lane * 16;
+        const uint8_t *g1 = row_ptr<const uint8_t>(s, r.o1) + a0 + lane * 16;
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d0), "l"(g0));
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d1), "l"(g1));
+      }
+      asm volatile("cp.async.commit_group;\n");
+    };
+    int o0[kPX], o1[kPX];
+#pragma unroll
+    for (int k = 0; k < kPX; k++) {
+      o0[k] = t[k].x - a0;
+      o1[k] = t[k].y - a0;
+    }
+#pragma unroll 1
+    for (int k = 0; k < kRing - 1; k++) issue(ybeg + k);
+#pragma unroll 1
+    for (int y = ybeg; y < yend; y++) {
+      issue(y + kRing - 1);
+      asm volatile("cp.async.wait_group %0;\n" ::"n"(kRing - 1));  // row y's copies (this lane's) landed
+      __syncwarp();                                                 // ... and every lane's
+      const LinTap r = yt[y];
+      const uint8_t *b0 = buf[y % kRing][0], *b1 = buf[y % kRing][1];
+      uint32_t out = 0;
+#pragma unroll
+      for (int k = 0; k < kPX; k++) out |= px(b0[o0[k]], b0[o1[k]], b1[o0[k]], b1[o1[k]], t[k], r.w0, r.w1) << (8 * k);
+      if (x < dw) put(d, y, x, dw, out);
+      __syncwarp();  // every lane has read slot y % kRing before it is refilled
+    }
+  }
+};
+
 struct LutArgs {
   int rows;
   const uint8_t *lut;
