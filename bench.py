@@ -722,6 +722,7 @@ def bench_served(args, ctx):
                 row["rounds"] = st["rounds"]
                 row["launches"] = st["launches"]
                 row["fallback_calls"] = st["fallback_calls"]
+                row["deferred"] = st["deferred"]
         results.append(row)
     results = results[1:]  # drop the warm-up run
     sat = results[-1]

@@ -46,6 +46,7 @@ typedef struct visar_server_stats {
     uint64_t fallback_calls;  /* per-call entry point calls */
     size_t pool_bytes, pool_used, pool_reserved;
     double mean_batch;        /* requests per stage group */
+    uint64_t deferred;        /* stage groups put off to a later round for pool or staging memory */
 } visar_server_stats;
 
 int visar_server_create(const visar_server_config *cfg, visar_server **out);

@@ -188,9 +188,10 @@ void set_tiles(const Launch &L, BImg &b) {
       b.tiles_y = (int)ceil_div(b.s.h, 8);
       break;
     case kOpGray: row_tiles(b, b.s.w, L.vec, L.rows, b.s.h); break;
+    case kOpCopy: row_tiles(b, (long long)b.s.w * b.s.cn * depth_size(L.depth), OpCopy::P, L.rows, b.s.h); break;
     case kOpHalf: row_tiles(b, b.d.w, L.vec, L.rows, b.d.h); break;
     case kOpLinear:
-      if (L.cn == 1) {  // OpLinearStrip warp tiles
+      if (L.cn == 1 && L.depth == k8U) {  // OpLinearStrip warp tiles
         b.tiles_x = (int)ceil_div(b.d.w, OpLinearStrip::kTW);
         b.tiles_y = (int)ceil_div(b.d.h, L.rows);
       } else {
@@ -242,7 +243,7 @@ void tune_and_tile(Launch &L, int num_sms) {
       retile();
       break;
     case kOpLinear:
-      if (L.cn == 1) {
+      if (L.cn == 1 && L.depth == k8U) {
         // Warp tiles: the tallest of 32..4 rows leaving ~8 tiles per warp slot.
         L.vec = 1;
         if (tuned > 0) {
@@ -258,12 +259,14 @@ void tune_and_tile(Launch &L, int num_sms) {
         break;
       }
       [[fallthrough]];
-    case kOpGray: case kOpHalf: case kOpLut: {
-      // Samples per thread (vector width): 8 or 16 bytes for gray and the
-      // LUT, 4 or 8 output pixels for the halving.
+    case kOpGray: case kOpHalf: case kOpLut: case kOpCopy: {
+      // Samples per thread (vector width): 8 or 16 bytes for u8 gray and the
+      // LUT, 4 or 8 output pixels for the halving (fixed for the others).
       const int vec = get("vec", -1);
       if (L.op == kOpHalf) L.vec = vec == 8 ? 8 : 4;
       else if (L.op == kOpLinear) L.vec = 1;
+      else if (L.op == kOpCopy) L.vec = OpCopy::P;
+      else if (L.op == kOpGray && L.depth == k32F) L.vec = OpGrayF<3>::P;
       else L.vec = vec == 8 ? 8 : 16;
       // Enough CTA tiles for ~8 per SM.
       L.rows = tuned > 0 ? std::min(tuned, 64) : 8;
@@ -336,6 +339,30 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
     if (m) std::memcpy(f.m, m, sizeof(double) * (st.kind == VISAR_STAGE_WARP_AFFINE ? 6 : 9));
     step.fallbacks.push_back(f);
   };
+  // u8 inputs whose rows are not 8-byte aligned (caller-owned images) are
+  // first copied, in one batched launch, into pitched pool images, so the
+  // stencil classes that need aligned rows take them instead of the per-call
+  // fallback.
+  std::vector<Buf> src(cur.begin(), cur.end());
+  auto repack_unaligned = [&]() -> int {
+    for (size_t i = 0; i < n; i++) {
+      const Buf &im = cur[i];
+      if (im.depth != k8U || u8_aligned8(im.v) || im.v.w < 2 || im.v.h < 2) continue;
+      if (im.v.cn != 1 && im.v.cn != 3 && im.v.cn != 4) continue;
+      Buf t;
+      if (!B.image(im.v.w, im.v.h, im.v.cn, im.depth, t)) return VISAR_OUT_OF_MEMORY;
+      Launch *l = class_of(ls, kOpCopy, im.depth, im.v.cn, 0, false);
+      add_img(l, bimg(im.v, t.v), im.input);
+      u8_bytes(*l, im.v, t.v, 1);
+      src[i] = t;
+    }
+    for (Launch &l : ls) {
+      tune_and_tile(l, B.P.num_sms);
+      step.launches.push_back(std::move(l));
+    }
+    ls.clear();
+    return VISAR_OK;
+  };
   switch (st.kind) {
     case VISAR_STAGE_GRAY: {
       for (size_t i = 0; i < n; i++) {
@@ -346,13 +373,13 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
         }
         if (im.v.cn != 3 && im.v.cn != 4) return VISAR_UNSUPPORTED;
         if (!B.image(im.v.w, im.v.h, 1, im.depth, next[i])) return VISAR_OUT_OF_MEMORY;
-        if (im.depth != k8U) {
+        if (im.depth != k8U && im.depth != k32F) {
           fallback(i, next[i], nullptr);
           continue;
         }
-        Launch *l = class_of(ls, kOpGray, k8U, im.v.cn, 0, false);
+        Launch *l = class_of(ls, kOpGray, im.depth, im.v.cn, 0, false);
         add_img(l, bimg(im.v, next[i].v), im.input);
-        u8_bytes(*l, im.v, next[i].v, 1);
+        u8_bytes(*l, im.v, next[i].v, depth_size(im.depth));
       }
       break;
     }
@@ -361,8 +388,9 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
       const double sx = st.d[0], sy = st.d[1] > 0 ? st.d[1] : st.d[0];
       if (border < 0 || border > 4) return VISAR_UNSUPPORTED;
       if (kw_in < 0 || kh_in < 0) return VISAR_INVALID_ARGUMENT;
+      if (const int rc = repack_unaligned(); rc != VISAR_OK) return rc;
       for (size_t i = 0; i < n; i++) {
-        const Buf &im = cur[i];
+        const Buf &im = src[i];
         if (!B.image(im.v.w, im.v.h, im.v.cn, im.depth, next[i])) return VISAR_OUT_OF_MEMORY;
         const bool u8 = im.depth == k8U;
         const int kw = kw_in > 0 ? kw_in : gaussian_ksize(sx, u8);
@@ -444,8 +472,11 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
       const int prof = row_profile(mask, kw, kh, dprof) ? strip::profile_of(dprof, kh) : strip::kProfileCount;
       std::vector<std::vector<Buf>> tmp(n);
       std::vector<int> mode(n, 0);  // 0 fallback, 1 strip passes, 2 fused strip, 3 band passes
+      if (kernel_ok) {
+        if (const int rc = repack_unaligned(); rc != VISAR_OK) return rc;
+      }
       for (size_t i = 0; i < n; i++) {
-        const Buf &im = cur[i];
+        const Buf &im = src[i];
         if (!B.image(im.v.w, im.v.h, im.v.cn, im.depth, next[i])) return VISAR_OUT_OF_MEMORY;
         const bool u8ok = kernel_ok && im.depth == k8U && (im.v.cn == 1 || im.v.cn == 3 || im.v.cn == 4) &&
                           u8_aligned4(im.v);
@@ -479,8 +510,8 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
         std::vector<Launch> pl;
         for (size_t i = 0; i < n; i++) {
           if (mode[i] != 1 && mode[i] != 3) continue;
-          const Buf &im = cur[i];
-          const DImg src = p == 0 ? im.v : tmp[i][(p - 1) % 2].v;
+          const Buf &im = src[i];
+          const DImg from = p == 0 ? im.v : tmp[i][(p - 1) % 2].v;
           const DImg dst = p + 1 == np ? next[i].v : tmp[i][p % 2].v;
           Launch *l;
           if (mode[i] == 1) {
@@ -489,8 +520,8 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
             l = class_of(pl, kOpMorph, k8U, im.v.cn, kh, passes[p]);
             fast::morph_fast_args(mask, kw, kh, im.v.cn, im.v.w, l->ma);
           }
-          add_img(l, bimg(src, dst), p == 0 ? im.input : -1);
-          u8_bytes(*l, src, dst, 1);
+          add_img(l, bimg(from, dst), p == 0 ? im.input : -1);
+          u8_bytes(*l, from, dst, 1);
         }
         for (Launch &l : pl) {
           tune_and_tile(l, B.P.num_sms);
@@ -515,6 +546,20 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
         }
         if (interp == 4) return VISAR_UNSUPPORTED;
         if (!B.image(dw, dh, im.v.cn, im.depth, next[i])) return VISAR_OUT_OF_MEMORY;
+        const bool f32lin = im.depth == k32F && im.v.cn <= 4 && interp == 1;
+        if (f32lin) {  // the generic f32 path (resize.zig:284-423), exact halves included
+          std::vector<FLinTap> xt(dw), yt(dh);
+          for (int x = 0; x < dw; x++) xt[x] = lin_tap_f(x, im.v.w, dw, false, true);
+          for (int y = 0; y < dh; y++) yt[y] = lin_tap_f(y, im.v.h, dh, false, false);
+          BImg b = bimg(im.v, next[i].v);
+          b.t0 = B.table(xt);
+          b.t1 = B.table(yt);
+          if (!B.sizing && (!b.t0 || !b.t1)) return VISAR_OUT_OF_MEMORY;
+          Launch *l = class_of(ls, kOpLinear, k32F, im.v.cn, 0, false);
+          add_img(l, b, im.input);
+          u8_bytes(*l, im.v, next[i].v, 4);
+          continue;
+        }
         const bool u8lin = im.depth == k8U && im.v.cn <= 4 && interp == 1;
         if (!u8lin) {
           fallback(i, next[i], nullptr);
@@ -731,13 +776,23 @@ cudaError_t run_launch(const Plan &P, const Launch &L, cudaStream_t st) {
       if (L.cn == 1) return run_morph<1>(P, L, st);
       if (L.cn == 3) return run_morph<3>(P, L, st);
       return run_morph<4>(P, L, st);
+    case kOpCopy: return run_op<OpCopy>(P, L, CopyArgs{L.rows, depth_size(L.depth)}, st);
     case kOpGray:
+      if (L.depth == k32F) return L.cn == 3 ? run_op<OpGrayF<3>>(P, L, ra, st) : run_op<OpGrayF<4>>(P, L, ra, st);
       if (L.vec == 8) return L.cn == 3 ? run_op<OpGray<3, 8>>(P, L, ra, st) : run_op<OpGray<4, 8>>(P, L, ra, st);
       return L.cn == 3 ? run_op<OpGray<3, 16>>(P, L, ra, st) : run_op<OpGray<4, 16>>(P, L, ra, st);
     case kOpHalf:
       if (L.vec == 8) return run_half<8>(P, L, ra, st);
       return run_half<4>(P, L, ra, st);
     case kOpLinear:
+      if (L.depth == k32F) {
+        switch (L.cn) {
+          case 1: return run_op<OpLinearF<1>>(P, L, ra, st);
+          case 2: return run_op<OpLinearF<2>>(P, L, ra, st);
+          case 3: return run_op<OpLinearF<3>>(P, L, ra, st);
+          default: return run_op<OpLinearF<4>>(P, L, ra, st);
+        }
+      }
       switch (L.cn) {
         case 1: return run_op<OpLinearStrip>(P, L, ra, st);
         case 2: return run_op<OpLinear<2>>(P, L, ra, st);

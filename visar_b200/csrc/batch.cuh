@@ -552,6 +552,102 @@ struct OpLut {
   }
 };
 
+// A byte copy of an image into a pitched pool image (any source alignment):
+// the batched form repacks inputs whose rows are not 8-byte aligned before
+// the stencils that need aligned rows. 16 bytes per thread.
+struct CopyArgs {
+  int rows;
+  int esize;  // bytes per sample
+};
+
+struct OpCopy {
+  static constexpr int kThreads = 256, kMinBlocks = 5, P = 16;
+  using Args = CopyArgs;
+  static size_t smem(const Args &) { return 0; }
+  static __device__ __forceinline__ void tile(const BImg &im, const Args &a, int tx, int ty, unsigned char *) {
+    const RowSpan r = row_span<kThreads, P>(im, a.rows, tx, ty, im.s.h);
+    const long long n = (long long)im.s.w * im.s.cn * a.esize;
+    if (r.x0 >= n) return;
+    const bool full = r.x0 + P <= n;
+    for (int y = r.y; y < r.yend; y += r.step) {
+      const uint8_t *sp = row_ptr<const uint8_t>(im.s, y) + r.x0;
+      uint8_t *dp = row_ptr<uint8_t>(im.d, y) + r.x0;
+      if (full && ((uintptr_t)dp & 15) == 0) {
+        uint4 v;
+        if (((uintptr_t)sp & 15) == 0) {
+          v = __ldg(reinterpret_cast<const uint4 *>(sp));
+        } else if (((uintptr_t)sp & 3) == 0) {
+          const uint32_t *w = reinterpret_cast<const uint32_t *>(sp);
+          v = make_uint4(__ldg(w), __ldg(w + 1), __ldg(w + 2), __ldg(w + 3));
+        } else {
+          uint32_t w[4];
+#pragma unroll
+          for (int q = 0; q < 4; q++)
+            w[q] = (uint32_t)__ldg(sp + 4 * q) | ((uint32_t)__ldg(sp + 4 * q + 1) << 8) |
+                   ((uint32_t)__ldg(sp + 4 * q + 2) << 16) | ((uint32_t)__ldg(sp + 4 * q + 3) << 24);
+          v = make_uint4(w[0], w[1], w[2], w[3]);
+        }
+        *reinterpret_cast<uint4 *>(dp) = v;
+      } else {
+        for (long long k = 0; k < P && r.x0 + k < n; k++) dp[k] = sp[k];
+      }
+    }
+  }
+};
+
+// f32 BGR / BGRA -> gray: b*0.114 + g*0.587 + r*0.299, unfused, in that
+// order (color.zig:400); 4 pixels per thread.
+template <int SCN>
+struct OpGrayF {
+  static constexpr int kThreads = 256, kMinBlocks = 4, P = 4;
+  using Args = RowArgs;
+  static size_t smem(const Args &) { return 0; }
+  static __device__ __forceinline__ void tile(const BImg &im, const Args &a, int tx, int ty, unsigned char *) {
+    const RowSpan r = row_span<kThreads, P>(im, a.rows, tx, ty, im.s.h);
+    const int w = im.s.w;
+    if (r.x0 >= w) return;
+    for (int y = r.y; y < r.yend; y += r.step) {
+      const float *sp = row_ptr<const float>(im.s, y) + (long long)r.x0 * SCN;
+      float *dp = row_ptr<float>(im.d, y) + r.x0;
+#pragma unroll
+      for (int i = 0; i < P; i++) {
+        if (r.x0 + i >= w) break;
+        const float *p = sp + i * SCN;
+        dp[i] = __fadd_rn(__fadd_rn(__fmul_rn(__ldg(p), 0.114f), __fmul_rn(__ldg(p + 1), 0.587f)),
+                          __fmul_rn(__ldg(p + 2), 0.299f));
+      }
+    }
+  }
+};
+
+// Generic bilinear for f32 (resize.zig:284-423): f32 weights, h = s0*a0 +
+// s1*a1, out = h0*b0 + h1*b1, unfused; one output pixel per thread.
+template <int CN>
+struct OpLinearF {
+  static constexpr int kThreads = 256, kMinBlocks = 4;
+  using Args = RowArgs;
+  static size_t smem(const Args &) { return 0; }
+  static __device__ __forceinline__ void tile(const BImg &im, const Args &a, int tx, int ty, unsigned char *) {
+    const RowSpan r = row_span<kThreads, 1>(im, a.rows, tx, ty, im.d.h);
+    const int x = r.x0;
+    if (x >= im.d.w) return;
+    const FLinTap tq = static_cast<const FLinTap *>(im.t0)[x];
+    const FLinTap *yt = static_cast<const FLinTap *>(im.t1);
+    const long long a0 = (long long)tq.o0 * CN, a1 = (long long)tq.o1 * CN;
+    for (int y = r.y; y < r.yend; y += r.step) {
+      const FLinTap t = yt[y];
+      const float *r0 = row_ptr<const float>(im.s, t.o0), *r1 = row_ptr<const float>(im.s, t.o1);
+      float *o = row_ptr<float>(im.d, y) + (long long)x * CN;
+#pragma unroll
+      for (int c = 0; c < CN; c++) {
+        const float h0 = __fadd_rn(__fmul_rn(__ldg(r0 + a0 + c), tq.a0), __fmul_rn(__ldg(r0 + a1 + c), tq.a1));
+        const float h1 = __fadd_rn(__fmul_rn(__ldg(r1 + a0 + c), tq.a0), __fmul_rn(__ldg(r1 + a1 + c), tq.a1));
+        o[c] = __fadd_rn(__fmul_rn(h0, t.a0), __fmul_rn(h1, t.a1));
+      }
+    }
+  }
+};
+
 // u8 Gaussian with binomial taps on warp strips (strip.cuh).
 template <int K, int CN, int RH>
 struct OpGaussStrip {

@@ -19,7 +19,10 @@ struct Buf {
   int input = -1;  // index of the plan input this buffer is, else -1
 };
 
-enum OpKind { kOpGauss, kOpMorph, kOpGray, kOpHalf, kOpLinear, kOpLut, kOpWarpAff, kOpWarpPer, kOpGaussStrip, kOpMorphStrip };
+enum OpKind {
+  kOpGauss, kOpMorph, kOpGray, kOpHalf, kOpLinear, kOpLut, kOpWarpAff, kOpWarpPer, kOpGaussStrip, kOpMorphStrip,
+  kOpCopy
+};
 
 inline const char *op_name(int op) {
   switch (op) {
@@ -33,6 +36,7 @@ inline const char *op_name(int op) {
     case kOpWarpPer: return "warp_perspective";
     case kOpGaussStrip: return "gauss_strip";
     case kOpMorphStrip: return "morph_strip";
+    case kOpCopy: return "copy";
   }
   return "?";
 }

@@ -17,6 +17,37 @@ int sat_i16(float x) {
   return (int)r;
 }
 
+// linearCoord + Weights(T).coef (resize.zig:156-179, 410-415).
+FLinTap lin_tap_f(long long d, uint32_t ssize, uint32_t dsize, bool area, bool is_x) {
+  const double scale = (double)ssize / (double)dsize;
+  long long sx;
+  double f;
+  if (area) {
+    const double df = (double)d;
+    sx = (long long)std::floor(df * scale);
+    f = (df + 1) - (double)(sx + 1) / scale;
+    f = f <= 0 ? 0 : f - std::floor(f);
+  } else {
+    const double fx = ((double)d + 0.5) * scale - 0.5;
+    sx = (long long)std::floor(fx);
+    f = fx - (double)sx;
+  }
+  if (sx < 0) {
+    sx = 0;
+    f = 0;
+  }
+  if (sx >= (long long)ssize - 1) {
+    sx = (long long)ssize - 1;
+    f = 0;
+  }
+  FLinTap t;
+  t.o0 = (int)sx;
+  t.o1 = is_x ? ((sx >= (long long)ssize - 1) ? (int)sx : (int)sx + 1) : (int)std::min(sx + 1, (long long)ssize - 1);
+  t.a0 = (float)(1.0 - f);
+  t.a1 = (float)f;
+  return t;
+}
+
 // linearTapU8 (src/imgproc/resize.zig:181-214): OpenCV's 8-bit bilinear taps, the
 // source coordinate in f32 and each weight rounded to 11 bits on its own.
 LinTap lin_tap_u8(long long d, uint32_t ssize, uint32_t dsize, bool area, bool pin) {

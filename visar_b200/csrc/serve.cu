@@ -167,6 +167,18 @@ struct Req {
   int state = 0;  // 0 queued, 1 admitted, 2 done, 3 released
   int status = VISAR_OK;
   std::string error;  // the failing call's message
+  struct Trace *trace = nullptr;  // trace replay: released by the scheduler when done
+  size_t trace_i = 0;
+};
+
+// A trace replay in progress: the scheduler records each request's latency
+// and releases it as soon as it completes (in completion order).
+struct Trace {
+  double *latency_ms = nullptr;
+  size_t done = 0;
+  double last_done = 0;
+  int rc = VISAR_OK;
+  std::string first_error;
 };
 
 struct Round {
@@ -211,6 +223,11 @@ struct visar_server {
   std::mutex mu;
   std::condition_variable cv_done;
   std::unordered_map<uint64_t, std::unique_ptr<Req>> reqs;
+  // Submissions wait here under their own lock (a submitter never waits for
+  // a scheduling round); the scheduler moves them into reqs / incoming.
+  std::mutex mu_in;
+  std::vector<std::unique_ptr<Req>> pending;
+  std::atomic<uint64_t> n_submitted{0};
   std::deque<uint64_t> incoming;
   std::vector<uint64_t> admitted;  // admitted, stages left
   std::deque<Round> rounds;        // in flight, oldest first
@@ -250,6 +267,50 @@ struct visar_server {
     return total + 2 * big;
   }
 
+  // Frees a completed request's result (mu held).
+  void release_locked(std::unordered_map<uint64_t, std::unique_ptr<Req>>::iterator it) {
+    Req &q = *it->second;
+    if (q.cur_owned) pool.free(q.cur.v.p);
+    reserved -= std::min(reserved, q.reserve);
+    reqs.erase(it);
+    stats.released++;
+  }
+
+  // A request has completed at time t (mu held): trace requests are recorded
+  // and released here.
+  void finished(uint64_t id, double t) {
+    auto it = reqs.find(id);
+    if (it == reqs.end()) return;
+    Req &q = *it->second;
+    q.state = 2;
+    q.t_done = t;
+    stats.completed++;
+    if (Trace *tr = q.trace) {
+      if (tr->latency_ms) tr->latency_ms[q.trace_i] = (q.t_done - q.t_submit) * 1e3;
+      tr->last_done = std::max(tr->last_done, q.t_done);
+      if (q.status != VISAR_OK && tr->rc == VISAR_OK) {
+        tr->rc = q.status;
+        tr->first_error = q.error;
+      }
+      tr->done++;
+      release_locked(it);
+    }
+  }
+
+  // Moves new submissions into the request table (takes mu_in; mu held).
+  void take_pending() {
+    std::vector<std::unique_ptr<Req>> got;
+    {
+      std::lock_guard<std::mutex> lk(mu_in);
+      got.swap(pending);
+    }
+    for (auto &q : got) {
+      incoming.push_back(q->id);
+      const uint64_t id = q->id;
+      reqs[id] = std::move(q);
+    }
+  }
+
   // Completed rounds: free their memory, finish their requests.
   void poll_rounds() {
     while (!rounds.empty()) {
@@ -262,14 +323,7 @@ struct visar_server {
       for (void *p : r.blocks) pool.free(p);
       if (r.staging) staging.release(r.staging, r.staging_end);
       const double t = now_s();
-      for (uint64_t id : r.finishing) {
-        auto it = reqs.find(id);
-        if (it == reqs.end()) continue;
-        Req &q = *it->second;
-        q.state = 2;
-        q.t_done = t;
-        stats.completed++;
-      }
+      for (uint64_t id : r.finishing) finished(id, t);
       for (auto &kv : reqs) {
         Req &q = *kv.second;
         if (q.ready == r.ev_launch || q.ready == r.ev_fb) q.ready = nullptr;
@@ -288,11 +342,11 @@ struct visar_server {
       q.reserve = reserve_for(q);
       if (q.reserve > budget) {  // can never fit the pool
         q.status = VISAR_OUT_OF_MEMORY;
-        q.state = 2;
-        q.t_done = now_s();
+        q.error = "OutOfMemory: request larger than the server pool";
         q.reserve = 0;
-        stats.completed++;
+        const uint64_t id = q.id;
         incoming.pop_front();
+        finished(id, now_s());
         cv_done.notify_all();
         continue;
       }
@@ -386,6 +440,7 @@ struct visar_server {
       }
       if (rc == VISAR_OUT_OF_MEMORY) {  // retry in a later round
         for (void *p : allocs) pool.free(p);
+        stats.deferred++;
         continue;
       }
       if (rc != VISAR_OK) {  // a stage the requests cannot run: fail them
@@ -563,6 +618,7 @@ struct visar_server {
       bool did = false;
       {
         std::lock_guard<std::mutex> lk(mu);
+        take_pending();
         poll_rounds();
         admit();
         if ((int)rounds.size() < cfg.max_inflight)
@@ -605,8 +661,8 @@ int visar_server_create(const visar_server_config *cfg, visar_server **out) {
   return VISAR_OK;
 }
 
-int visar_server_submit(visar_server *s, const visar_image *input, const visar_stage *stages, size_t nstages,
-                        uint64_t *id) {
+static int submit_req(visar_server *s, const visar_image *input, const visar_stage *stages, size_t nstages,
+                      uint64_t *id, Trace *trace, size_t trace_i) {
   if (!s || !input || !input->data || !stages || nstages == 0 || nstages > 16 || !id)
     return report_error(VISAR_INVALID_ARGUMENT, "InvalidArgument");
   if (!(input->depth == 0 || input->depth == 2 || input->depth == 3 || input->depth == 5))
@@ -627,22 +683,45 @@ int visar_server_submit(visar_server *s, const visar_image *input, const visar_s
     for (int j = 0; j < nm; j++) q->mats[k][j] = st.per_image ? st.per_image[j] : st.d[j];
     q->st[k].per_image = nullptr;
   }
+  q->trace = trace;
+  q->trace_i = trace_i;
   q->t_submit = now_s();
-  std::lock_guard<std::mutex> lk(s->mu);
+  std::lock_guard<std::mutex> lk(s->mu_in);
   q->id = s->next_id++;
   *id = q->id;
-  s->incoming.push_back(q->id);
-  s->reqs[q->id] = std::move(q);
-  s->stats.submitted++;
+  s->pending.push_back(std::move(q));
+  s->n_submitted++;
   return VISAR_OK;
+}
+
+// The request with this id (mu held), or nullptr; *queued = true when it is
+// still in the submission queue.
+static Req *find_req(visar_server *s, uint64_t id, bool *queued) {
+  *queued = false;
+  auto it = s->reqs.find(id);
+  if (it != s->reqs.end()) return it->second.get();
+  std::lock_guard<std::mutex> lk(s->mu_in);
+  for (auto &q : s->pending)
+    if (q->id == id) *queued = true;
+  return nullptr;
+}
+
+int visar_server_submit(visar_server *s, const visar_image *input, const visar_stage *stages, size_t nstages,
+                        uint64_t *id) {
+  return submit_req(s, input, stages, nstages, id, nullptr, 0);
 }
 
 int visar_server_poll(visar_server *s, uint64_t id, int *done, visar_image *out) {
   if (!s || !done) return report_error(VISAR_INVALID_ARGUMENT, "InvalidArgument");
   std::lock_guard<std::mutex> lk(s->mu);
-  auto it = s->reqs.find(id);
-  if (it == s->reqs.end() || it->second->state == 3) return report_error(VISAR_INVALID_ARGUMENT, "InvalidArgument: request id");
-  Req &q = *it->second;
+  bool queued;
+  Req *r = find_req(s, id, &queued);
+  if (queued) {
+    *done = 0;
+    return VISAR_OK;
+  }
+  if (!r || r->state == 3 || r->trace) return report_error(VISAR_INVALID_ARGUMENT, "InvalidArgument: request id");
+  Req &q = *r;
   *done = q.state == 2;
   if (*done && out) *out = cimg(q.cur);
   if (*done && q.status != VISAR_OK) return report_error(q.status, q.error.empty() ? "request failed" : q.error.c_str());
@@ -653,9 +732,14 @@ int visar_server_wait(visar_server *s, uint64_t id, visar_image *out) {
   if (!s) return report_error(VISAR_INVALID_ARGUMENT, "InvalidArgument");
   std::unique_lock<std::mutex> lk(s->mu);
   for (;;) {
-    auto it = s->reqs.find(id);
-    if (it == s->reqs.end() || it->second->state == 3) return report_error(VISAR_INVALID_ARGUMENT, "InvalidArgument: request id");
-    Req &q = *it->second;
+    bool queued;
+    Req *r = find_req(s, id, &queued);
+    if (queued) {
+      s->cv_done.wait_for(lk, std::chrono::milliseconds(1));
+      continue;
+    }
+    if (!r || r->state == 3 || r->trace) return report_error(VISAR_INVALID_ARGUMENT, "InvalidArgument: request id");
+    Req &q = *r;
     if (q.state == 2) {
       if (out) *out = cimg(q.cur);
       return q.status == VISAR_OK ? VISAR_OK : report_error(q.status, q.error.empty() ? "request failed" : q.error.c_str());
@@ -668,12 +752,9 @@ int visar_server_release(visar_server *s, uint64_t id) {
   if (!s) return report_error(VISAR_INVALID_ARGUMENT, "InvalidArgument");
   std::lock_guard<std::mutex> lk(s->mu);
   auto it = s->reqs.find(id);
-  if (it == s->reqs.end() || it->second->state != 2) return report_error(VISAR_INVALID_ARGUMENT, "InvalidArgument: request not done");
-  Req &q = *it->second;
-  if (q.cur_owned) s->pool.free(q.cur.v.p);
-  s->reserved -= std::min(s->reserved, q.reserve);
-  s->reqs.erase(it);
-  s->stats.released++;
+  if (it == s->reqs.end() || it->second->state != 2 || it->second->trace)
+    return report_error(VISAR_INVALID_ARGUMENT, "InvalidArgument: request not done");
+  s->release_locked(it);
   return VISAR_OK;
 }
 
@@ -681,6 +762,7 @@ int visar_server_get_stats(visar_server *s, visar_server_stats *st) {
   if (!s || !st) return report_error(VISAR_INVALID_ARGUMENT, "InvalidArgument");
   std::lock_guard<std::mutex> lk(s->mu);
   *st = s->stats;
+  st->submitted = s->n_submitted.load();
   st->pool_used = s->pool.used();
   st->pool_reserved = s->reserved;
   st->mean_batch = s->groups ? (double)s->grouped / (double)s->groups : 0.0;
@@ -707,10 +789,13 @@ void visar_server_destroy(visar_server *s) {
 int visar_server_run_trace(visar_server *s, const visar_trace_request *reqs, size_t n, double *latency_ms,
                            double *elapsed_s) {
   if (!s || (n > 0 && !reqs)) return report_error(VISAR_INVALID_ARGUMENT, "InvalidArgument");
-  std::vector<std::atomic<uint64_t>> ids(n);
-  for (auto &a : ids) a.store(0);
+  Trace tr;
+  tr.latency_ms = latency_ms;
+  std::atomic<size_t> submitted{0};
   std::atomic<int> submit_rc{VISAR_OK};
+  std::string submit_error;
   const double t0 = now_s();
+  tr.last_done = t0;
   std::thread submitter([&] {
     cudaSetDevice(s->dev);
     for (size_t i = 0; i < n; i++) {
@@ -718,50 +803,25 @@ int visar_server_run_trace(visar_server *s, const visar_trace_request *reqs, siz
       for (double t = now_s(); t < due; t = now_s())
         if (due - t > 200e-6) std::this_thread::sleep_for(std::chrono::microseconds(50));
       uint64_t id = 0;
-      const int rc = visar_server_submit(s, &reqs[i].input, reqs[i].stages, reqs[i].nstages, &id);
+      const int rc = submit_req(s, &reqs[i].input, reqs[i].stages, reqs[i].nstages, &id, &tr, i);
       if (rc != VISAR_OK) {
+        if (submit_rc.load() == VISAR_OK) submit_error = visar_last_error();
         submit_rc.store(rc);
-        id = ~0ull;
+        if (latency_ms) latency_ms[i] = -1;
+        continue;
       }
-      ids[i].store(id);
+      submitted++;
     }
   });
-  double last_done = t0;
-  int rc = VISAR_OK;
-  std::string first_error;
-  for (size_t i = 0; i < n; i++) {
-    uint64_t id;
-    while ((id = ids[i].load()) == 0) std::this_thread::sleep_for(std::chrono::microseconds(20));
-    if (id == ~0ull) {
-      if (latency_ms) latency_ms[i] = -1;
-      continue;
-    }
-    for (;;) {
-      std::unique_lock<std::mutex> lk(s->mu);
-      auto it = s->reqs.find(id);
-      if (it == s->reqs.end()) {
-        rc = VISAR_INTERNAL;
-        break;
-      }
-      Req &q = *it->second;
-      if (q.state == 2) {
-        if (latency_ms) latency_ms[i] = (q.t_done - q.t_submit) * 1e3;
-        last_done = std::max(last_done, q.t_done);
-        if (q.status != VISAR_OK) {
-          rc = q.status;
-          if (first_error.empty()) first_error = q.error;
-        }
-        lk.unlock();
-        visar_server_release(s, id);
-        break;
-      }
-      s->cv_done.wait_for(lk, std::chrono::milliseconds(2));
-    }
-  }
   submitter.join();
-  if (elapsed_s) *elapsed_s = last_done - (t0 + (n ? reqs[0].arrival_s : 0.0));
-  if (submit_rc.load() != VISAR_OK) return submit_rc.load();
-  return rc == VISAR_OK ? VISAR_OK : report_error(rc, first_error.empty() ? "a request failed" : first_error.c_str());
+  {
+    std::unique_lock<std::mutex> lk(s->mu);
+    while (tr.done < submitted.load()) s->cv_done.wait_for(lk, std::chrono::milliseconds(2));
+  }
+  if (elapsed_s) *elapsed_s = tr.last_done - (t0 + (n ? reqs[0].arrival_s : 0.0));
+  if (submit_rc.load() != VISAR_OK) return report_error(submit_rc.load(), submit_error.c_str());
+  return tr.rc == VISAR_OK ? VISAR_OK
+                           : report_error(tr.rc, tr.first_error.empty() ? "a request failed" : tr.first_error.c_str());
 }
 
 }  // extern "C"

@@ -118,6 +118,8 @@ bool deriv_kernel(int *out, int n, int order, int ksize);
 int sat_i16(float x);
 // linearTapU8 (src/imgproc/resize.zig:181-214) for destination index d.
 LinTap lin_tap_u8(long long d, uint32_t ssize, uint32_t dsize, bool area, bool pin);
+// linearCoord + Weights(T).coef (src/imgproc/resize.zig:156-179, 410-415): generic bilinear taps.
+FLinTap lin_tap_f(long long d, uint32_t ssize, uint32_t dsize, bool area, bool is_x);
 // getStructuringElement (src/imgproc/morph.zig:32-59): h x w mask, row-major.
 std::vector<uint8_t> structuring_element(int shape, int w, int h);
 // warpAffine's inverse map in f32 / warpPerspective's in f64; false if singular.
