@@ -46,6 +46,8 @@ CANDIDATES = {
     "lut": {"rows": (1, 2, 4, 8, 16), "vec": (8, 16), "per_sm": (2, 4, 6)},
     "half": {"rows": (1, 2, 4, 8, 16), "vec": (4, 8), "per_sm": (2, 4, 6)},
     "linear": {"rows": (2, 4, 8, 16, 32), "per_sm": (2, 4, 6)},
+    "morph_f": {"rows": (1, 2, 4, 8, 16), "per_sm": (2, 4)},
+    "copy": {"rows": (1, 2, 4, 8, 16), "per_sm": (2, 4)},
     "warp_affine": {"per_sm": (2, 4, 8)},
     "warp_perspective": {"per_sm": (2, 4, 8)},
 }

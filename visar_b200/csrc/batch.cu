@@ -81,7 +81,7 @@ std::string size_class(const std::vector<BImg> &imgs) {
 }
 
 const char *launch_suffix(const Launch &L) {
-  if (L.op != kOpMorph && L.op != kOpMorphStrip) return "";
+  if (L.op != kOpMorph && L.op != kOpMorphStrip && L.op != kOpMorphF) return "";
   if (L.fused) return L.is_max ? ".close" : ".open";
   return L.is_max ? ".max" : ".min";
 }
@@ -189,6 +189,7 @@ void set_tiles(const Launch &L, BImg &b) {
       break;
     case kOpGray: row_tiles(b, b.s.w, L.vec, L.rows, b.s.h); break;
     case kOpCopy: row_tiles(b, (long long)b.s.w * b.s.cn * depth_size(L.depth), OpCopy::P, L.rows, b.s.h); break;
+    case kOpMorphF: row_tiles(b, b.s.w, 1, L.rows, b.s.h); break;
     case kOpHalf: row_tiles(b, b.d.w, L.vec, L.rows, b.d.h); break;
     case kOpLinear:
       if (L.cn == 1 && L.depth == k8U) {  // OpLinearStrip warp tiles
@@ -259,13 +260,14 @@ void tune_and_tile(Launch &L, int num_sms) {
         break;
       }
       [[fallthrough]];
-    case kOpGray: case kOpHalf: case kOpLut: case kOpCopy: {
+    case kOpGray: case kOpHalf: case kOpLut: case kOpCopy: case kOpMorphF: {
       // Samples per thread (vector width): 8 or 16 bytes for u8 gray and the
       // LUT, 4 or 8 output pixels for the halving (fixed for the others).
       const int vec = get("vec", -1);
       if (L.op == kOpHalf) L.vec = vec == 8 ? 8 : 4;
       else if (L.op == kOpLinear) L.vec = 1;
       else if (L.op == kOpCopy) L.vec = OpCopy::P;
+      else if (L.op == kOpMorphF) L.vec = 1;
       else if (L.op == kOpGray && L.depth == k32F) L.vec = OpGrayF<3>::P;
       else L.vec = vec == 8 ? 8 : 16;
       // Enough CTA tiles for ~8 per SM.
@@ -471,7 +473,8 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
       int dprof[16];
       const int prof = row_profile(mask, kw, kh, dprof) ? strip::profile_of(dprof, kh) : strip::kProfileCount;
       std::vector<std::vector<Buf>> tmp(n);
-      std::vector<int> mode(n, 0);  // 0 fallback, 1 strip passes, 2 fused strip, 3 band passes
+      std::vector<int> mode(n, 0);  // 0 fallback, 1 strip passes, 2 fused strip, 3 band passes, 4 f32 rectangle passes
+      const bool rect = std::all_of(mask.begin(), mask.end(), [](uint8_t m) { return m != 0; });
       if (kernel_ok) {
         if (const int rc = repack_unaligned(); rc != VISAR_OK) return rc;
       }
@@ -491,6 +494,7 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
         }
         if (strip_ok) mode[i] = 1;
         else if (u8ok && fast::morph_fast_args(mask, kw, kh, im.v.cn, im.v.w, ma)) mode[i] = 3;
+        else if (kernel_ok && im.depth == k32F && rect && kw <= 15 && kh <= 15 && im.v.cn <= 4) mode[i] = 4;
         if (mode[i] == 0) {
           fallback(i, next[i], nullptr);
           continue;
@@ -509,19 +513,21 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
       for (size_t p = 0; p < np && kernel_ok; p++) {
         std::vector<Launch> pl;
         for (size_t i = 0; i < n; i++) {
-          if (mode[i] != 1 && mode[i] != 3) continue;
+          if (mode[i] != 1 && mode[i] != 3 && mode[i] != 4) continue;
           const Buf &im = src[i];
           const DImg from = p == 0 ? im.v : tmp[i][(p - 1) % 2].v;
           const DImg dst = p + 1 == np ? next[i].v : tmp[i][p % 2].v;
           Launch *l;
           if (mode[i] == 1) {
             l = class_of(pl, kOpMorphStrip, k8U, im.v.cn, kh, passes[p], false, prof);
+          } else if (mode[i] == 4) {
+            l = class_of(pl, kOpMorphF, k32F, im.v.cn, kh, passes[p], false, kw);
           } else {
             l = class_of(pl, kOpMorph, k8U, im.v.cn, kh, passes[p]);
             fast::morph_fast_args(mask, kw, kh, im.v.cn, im.v.w, l->ma);
           }
           add_img(l, bimg(from, dst), p == 0 ? im.input : -1);
-          u8_bytes(*l, from, dst, 1);
+          u8_bytes(*l, from, dst, depth_size(im.depth));
         }
         for (Launch &l : pl) {
           tune_and_tile(l, B.P.num_sms);
@@ -777,6 +783,15 @@ cudaError_t run_launch(const Plan &P, const Launch &L, cudaStream_t st) {
       if (L.cn == 3) return run_morph<3>(P, L, st);
       return run_morph<4>(P, L, st);
     case kOpCopy: return run_op<OpCopy>(P, L, CopyArgs{L.rows, depth_size(L.depth)}, st);
+    case kOpMorphF: {
+      const MorphFArgs a{L.rows, L.sub, L.k, L.is_max};
+      switch (L.cn) {
+        case 1: return run_op<OpMorphF<1>>(P, L, a, st);
+        case 2: return run_op<OpMorphF<2>>(P, L, a, st);
+        case 3: return run_op<OpMorphF<3>>(P, L, a, st);
+        default: return run_op<OpMorphF<4>>(P, L, a, st);
+      }
+    }
     case kOpGray:
       if (L.depth == k32F) return L.cn == 3 ? run_op<OpGrayF<3>>(P, L, ra, st) : run_op<OpGrayF<4>>(P, L, ra, st);
       if (L.vec == 8) return L.cn == 3 ? run_op<OpGray<3, 8>>(P, L, ra, st) : run_op<OpGray<4, 8>>(P, L, ra, st);

@@ -648,6 +648,48 @@ struct OpLinearF {
   }
 };
 
+struct MorphFArgs {
+  int rows;
+  int kw, kh;  // rectangle, anchored at its centre
+  bool is_max;
+};
+
+// f32 erode / dilate with a kw x kh rectangle, one pixel (all channels) per
+// thread reading its window directly; pixels outside the image are ignored
+// (morph.zig:473-474: the identity), min / max as fminf / fmaxf.
+template <int CN>
+struct OpMorphF {
+  static constexpr int kThreads = 256, kMinBlocks = 4;
+  using Args = MorphFArgs;
+  static size_t smem(const Args &) { return 0; }
+  static __device__ __forceinline__ void tile(const BImg &im, const Args &a, int tx, int ty, unsigned char *) {
+    const RowSpan r = row_span<kThreads, 1>(im, a.rows, tx, ty, im.s.h);
+    const int x = r.x0, w = im.s.w, h = im.s.h;
+    if (x >= w) return;
+    const int xs0 = max(0, x - a.kw / 2), xs1 = min(w - 1, x - a.kw / 2 + a.kw - 1);
+    const float id = a.is_max ? -__int_as_float(0x7f800000) : __int_as_float(0x7f800000);
+    for (int y = r.y; y < r.yend; y += r.step) {
+      const int ys0 = max(0, y - a.kh / 2), ys1 = min(h - 1, y - a.kh / 2 + a.kh - 1);
+      float v[CN];
+#pragma unroll
+      for (int c = 0; c < CN; c++) v[c] = id;
+      for (int sy = ys0; sy <= ys1; sy++) {
+        const float *row = row_ptr<const float>(im.s, sy);
+        for (int sx = xs0; sx <= xs1; sx++) {
+#pragma unroll
+          for (int c = 0; c < CN; c++) {
+            const float u = __ldg(row + (long long)sx * CN + c);
+            v[c] = a.is_max ? fmaxf(v[c], u) : fminf(v[c], u);
+          }
+        }
+      }
+      float *o = row_ptr<float>(im.d, y) + (long long)x * CN;
+#pragma unroll
+      for (int c = 0; c < CN; c++) o[c] = v[c];
+    }
+  }
+};
+
 // u8 Gaussian with binomial taps on warp strips (strip.cuh).
 template <int K, int CN, int RH>
 struct OpGaussStrip {

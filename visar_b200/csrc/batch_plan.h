@@ -21,7 +21,7 @@ struct Buf {
 
 enum OpKind {
   kOpGauss, kOpMorph, kOpGray, kOpHalf, kOpLinear, kOpLut, kOpWarpAff, kOpWarpPer, kOpGaussStrip, kOpMorphStrip,
-  kOpCopy
+  kOpCopy, kOpMorphF
 };
 
 inline const char *op_name(int op) {
@@ -37,6 +37,7 @@ inline const char *op_name(int op) {
     case kOpGaussStrip: return "gauss_strip";
     case kOpMorphStrip: return "morph_strip";
     case kOpCopy: return "copy";
+    case kOpMorphF: return "morph_f";
   }
   return "?";
 }
