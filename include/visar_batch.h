@@ -93,10 +93,17 @@ void visar_batch_destroy(visar_batch *b);
    video frame). Enqueued on the run stream (a one-thread kernel patches the
    device descriptors), so graph replays see it. */
 int visar_batch_set_input(visar_batch *b, size_t i, const visar_image *img);
-/* Host <-> device copies of all inputs / final outputs (one 2-D copy per
-   image, from or to `host[i]`, which must match the image's shape; pinned
-   host memory keeps them asynchronous). Same stream and async rules as
-   visar_batch_run. */
+/* Host <-> device copies of all inputs / final outputs, from or to `host[i]`,
+   which must match the image's shape; pinned host memory keeps them
+   asynchronous. When every host image's rows are contiguous (stride = row
+   bytes), each image crosses PCIe as one 1-D copy into (out of) a plan-owned
+   device staging buffer and a kernel restrides it into (out of) the pitched
+   plan images; 2-D copies of short pitched rows run at about half the link
+   rate. The staging buffer and its table are allocated on the first such
+   call (and again when the images change). Otherwise one 2-D copy per image.
+   Same stream and async rules as visar_batch_run; a plan's uploads (and its
+   downloads) share one staging buffer, so they must not overlap on
+   different streams. */
 int visar_batch_upload(visar_batch *b, const visar_image *host, size_t n);
 int visar_batch_download(visar_batch *b, const visar_image *host, size_t n);
 

@@ -912,6 +912,115 @@ int finish(cudaStream_t st) {
 using namespace vb;
 using namespace vb::bt;
 
+namespace vb {
+namespace bt {
+
+// Rows of one image per warp, 16 bytes per lane: source words are read
+// aligned and funnel-shifted (never past the row), destination written as
+// one 16-byte store when aligned, else by words or bytes.
+__global__ void __launch_bounds__(256) k_restride(const StageCopy *t, int n) {
+  const int i = blockIdx.y;
+  if (i >= n) return;
+  const StageCopy c = t[i];
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < c.h; r += warps) {
+    const uint8_t *s = c.src + (long long)r * c.sstride;
+    uint8_t *d = c.dst + (long long)r * c.dstride;
+    for (int x = lane * 16; x < c.rb; x += 32 * 16) {
+      if (x + 20 <= c.rb) {
+        const uintptr_t a = (uintptr_t)(s + x);
+        const uint32_t *w = reinterpret_cast<const uint32_t *>(a & ~(uintptr_t)3);
+        const uint32_t sh = (uint32_t)(a & 3) * 8;
+        uint32_t q[5];
+#pragma unroll
+        for (int k = 0; k < 5; k++) q[k] = __ldg(w + k);
+        uint32_t o[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) o[k] = __funnelshift_r(q[k], q[k + 1], sh);
+        uint8_t *p = d + x;
+        if (((uintptr_t)p & 15) == 0) {
+          *reinterpret_cast<uint4 *>(p) = make_uint4(o[0], o[1], o[2], o[3]);
+        } else if (((uintptr_t)p & 3) == 0) {
+#pragma unroll
+          for (int k = 0; k < 4; k++) reinterpret_cast<uint32_t *>(p)[k] = o[k];
+        } else {
+#pragma unroll
+          for (int k = 0; k < 16; k++) p[k] = (uint8_t)(o[k >> 2] >> (8 * (k & 3)));
+        }
+      } else {
+        for (int k = x; k < c.rb && k < x + 16; k++) d[k] = s[k];
+      }
+    }
+  }
+}
+
+namespace {
+
+// Staged transfers apply when every host image's rows are contiguous and
+// the plan has at most 65535 images (one grid row each).
+bool staged_ok(const visar_image *host, size_t n, const std::vector<StageCopy> &imgs) {
+  if (n == 0 || n > 65535) return false;
+  for (size_t i = 0; i < n; i++)
+    if ((long long)host[i].stride != (long long)imgs[i].rb) return false;
+  return true;
+}
+
+// Builds (or reuses) the staging buffer and the restride table for these
+// images; `in`: staging -> plan images, else plan images -> staging. The
+// table is rebuilt (a synchronous upload) only when the images changed.
+int staging_prepare(XferStaging &S, std::vector<StageCopy> &imgs, bool in) {
+  size_t total = 0;
+  std::vector<size_t> off(imgs.size());
+  for (size_t i = 0; i < imgs.size(); i++) {
+    off[i] = total;
+    total += ((size_t)imgs[i].rb * imgs[i].h + 255) & ~(size_t)255;
+  }
+  bool same = S.buf != nullptr && S.rows.size() == imgs.size();
+  for (size_t i = 0; same && i < imgs.size(); i++) {
+    const StageCopy &a = S.rows[i], &b = imgs[i];
+    same = (in ? a.dst == b.dst && a.dstride == b.dstride : a.src == b.src && a.sstride == b.sstride) && a.rb == b.rb &&
+           a.h == b.h;
+  }
+  if (same) return VISAR_OK;
+  if (S.buf) cudaFree(S.buf);
+  if (S.table) cudaFree(S.table);
+  S.buf = nullptr;
+  S.table = nullptr;
+  S.rows.clear();
+  cudaError_t e = cudaMalloc(&S.buf, std::max<size_t>(total, 256));
+  if (e == cudaSuccess) e = cudaMalloc(&S.table, sizeof(StageCopy) * imgs.size());
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    if (S.buf) cudaFree(S.buf);
+    S.buf = nullptr;
+    return report_error(VISAR_OUT_OF_MEMORY, "OutOfMemory: transfer staging");
+  }
+  S.maxh = 0;
+  for (size_t i = 0; i < imgs.size(); i++) {
+    if (in) imgs[i].src = S.buf + off[i];
+    else imgs[i].dst = S.buf + off[i];
+    S.maxh = std::max(S.maxh, imgs[i].h);
+  }
+  if ((e = cudaMemcpy(S.table, imgs.data(), sizeof(StageCopy) * imgs.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
+    return cuda_status(e);
+  S.rows = imgs;
+  S.off = off;
+  return VISAR_OK;
+}
+
+cudaError_t launch_restride(const XferStaging &S, cudaStream_t st) {
+  const int n = (int)S.rows.size();
+  const int gx = std::max(1, std::min(64, (S.maxh + 7) / 8));
+  k_restride<<<dim3(gx, n), 256, 0, st>>>(S.table, n);
+  note_launch();
+  return cudaGetLastError();
+}
+
+}  // namespace
+}  // namespace bt
+}  // namespace vb
+
 struct visar_batch {
   Plan plan;
 };
@@ -1147,11 +1256,28 @@ int visar_batch_upload(visar_batch *b, const visar_image *host, size_t n) {
   cudaError_t e = cudaSetDevice(P.dev);
   if (e != cudaSuccess) return cuda_status(e);
   const cudaStream_t st = run_stream(P);
+  for (size_t i = 0; i < n; i++)
+    if (!host[i].data || !same_shape(host[i], P.inputs[i])) return report_error(VISAR_SIZE_MISMATCH, "SizeMismatch");
+  std::vector<StageCopy> imgs(n);
   for (size_t i = 0; i < n; i++) {
     const Buf &d = P.inputs[i];
-    if (!host[i].data || !same_shape(host[i], d)) return report_error(VISAR_SIZE_MISMATCH, "SizeMismatch");
-    const size_t rb = (size_t)d.v.w * d.v.cn * depth_size(d.depth);
-    e = cudaMemcpy2DAsync(d.v.p, (size_t)d.v.stride, host[i].data, host[i].stride, rb, (size_t)d.v.h, cudaMemcpyHostToDevice, st);
+    const int rb = d.v.w * d.v.cn * depth_size(d.depth);
+    imgs[i] = StageCopy{nullptr, d.v.p, rb, (long long)d.v.stride, rb, d.v.h};
+  }
+  if (staged_ok(host, n, imgs)) {
+    const int rc = staging_prepare(P.up, imgs, true);
+    if (rc != VISAR_OK) return rc;
+    for (size_t i = 0; i < n; i++) {
+      e = cudaMemcpyAsync(P.up.buf + P.up.off[i], host[i].data, (size_t)imgs[i].rb * imgs[i].h, cudaMemcpyHostToDevice, st);
+      if (e != cudaSuccess) return cuda_status(e);
+    }
+    if ((e = launch_restride(P.up, st)) != cudaSuccess) return cuda_status(e);
+    return finish(st);
+  }
+  for (size_t i = 0; i < n; i++) {
+    const Buf &d = P.inputs[i];
+    e = cudaMemcpy2DAsync(d.v.p, (size_t)d.v.stride, host[i].data, host[i].stride, (size_t)imgs[i].rb, (size_t)d.v.h,
+                          cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return cuda_status(e);
   }
   return finish(st);
@@ -1163,11 +1289,27 @@ int visar_batch_download(visar_batch *b, const visar_image *host, size_t n) {
   cudaError_t e = cudaSetDevice(P.dev);
   if (e != cudaSuccess) return cuda_status(e);
   const cudaStream_t st = run_stream(P);
+  std::vector<StageCopy> imgs(n);
   for (size_t i = 0; i < n; i++) {
     const Buf &s = P.outs.empty() ? P.inputs[i] : P.outs.back()[i];
     if (!host[i].data || !same_shape(host[i], s)) return report_error(VISAR_SIZE_MISMATCH, "SizeMismatch");
-    const size_t rb = (size_t)s.v.w * s.v.cn * depth_size(s.depth);
-    e = cudaMemcpy2DAsync(host[i].data, host[i].stride, s.v.p, (size_t)s.v.stride, rb, (size_t)s.v.h, cudaMemcpyDeviceToHost, st);
+    const int rb = s.v.w * s.v.cn * depth_size(s.depth);
+    imgs[i] = StageCopy{s.v.p, nullptr, (long long)s.v.stride, rb, rb, s.v.h};
+  }
+  if (staged_ok(host, n, imgs)) {
+    const int rc = staging_prepare(P.down, imgs, false);
+    if (rc != VISAR_OK) return rc;
+    if ((e = launch_restride(P.down, st)) != cudaSuccess) return cuda_status(e);
+    for (size_t i = 0; i < n; i++) {
+      e = cudaMemcpyAsync(host[i].data, P.down.buf + P.down.off[i], (size_t)imgs[i].rb * imgs[i].h, cudaMemcpyDeviceToHost, st);
+      if (e != cudaSuccess) return cuda_status(e);
+    }
+    return finish(st);
+  }
+  for (size_t i = 0; i < n; i++) {
+    const Buf &s = P.outs.empty() ? P.inputs[i] : P.outs.back()[i];
+    e = cudaMemcpy2DAsync(host[i].data, host[i].stride, s.v.p, (size_t)s.v.stride, (size_t)imgs[i].rb, (size_t)s.v.h,
+                          cudaMemcpyDeviceToHost, st);
     if (e != cudaSuccess) return cuda_status(e);
   }
   return finish(st);

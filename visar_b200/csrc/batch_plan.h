@@ -95,6 +95,30 @@ struct Pool {
   }
 };
 
+// One image of a restriding copy (contiguous host-copy staging <-> pitched
+// plan images): rb bytes per row, h rows.
+struct StageCopy {
+  const uint8_t *src;
+  uint8_t *dst;
+  long long sstride, dstride;
+  int rb, h;
+};
+
+// Device staging for host transfers: the images laid out contiguously, so
+// each image crosses PCIe as one 1D copy (2D copies of short pitched rows
+// run at about half the link rate), then a kernel restrides them.
+struct XferStaging {
+  uint8_t *buf = nullptr;
+  StageCopy *table = nullptr;          // device copy of `rows`
+  std::vector<StageCopy> rows;         // as built (pitched side per image)
+  std::vector<size_t> off;             // image offsets in buf
+  int maxh = 0;
+  ~XferStaging() {
+    if (buf) cudaFree(buf);
+    if (table) cudaFree(table);
+  }
+};
+
 struct Plan {
   int dev = 0;
   int num_sms = 148;
@@ -110,6 +134,7 @@ struct Plan {
   bool prof = false;
   bool prof_valid = false;
   std::vector<cudaEvent_t> evs;  // 2 per launch when profiling
+  XferStaging up, down;          // visar_batch_upload / _download
   ~Plan() {
     for (cudaEvent_t e : evs) cudaEventDestroy(e);
     if (graph) cudaGraphExecDestroy(graph);
