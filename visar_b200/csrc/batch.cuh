@@ -238,7 +238,7 @@ __device__ __forceinline__ uint32_t gray_px(uint32_t b, uint32_t g, uint32_t r) 
 // thread.
 template <int SCN, int P>
 struct OpGray {
-  static constexpr int kThreads = 256, kMinBlocks = P == 16 ? 4 : 5;  // <= 64 / 48 registers
+  static constexpr int kThreads = 256, kMinBlocks = P == 16 || SCN == 4 ? 4 : 5;  // <= 64 / 48 registers
   using Args = RowArgs;
   static size_t smem(const Args &) { return 0; }
   static __device__ __forceinline__ void px(const Vb<P, SCN> &in, Vb<P, 1> &out) {
@@ -253,31 +253,44 @@ struct OpGray {
       out.word(q) = w;
     }
   }
+  // U rows per thread in flight (their loads issued together): 4 with 8
+  // pixels per thread, 2 with 16.
+  static constexpr int U = P == 8 ? 4 : 2;
   static __device__ __forceinline__ void tile(const BImg &im, const Args &a, int tx, int ty, unsigned char *) {
     const RowSpan r = row_span<kThreads, P>(im, a.rows, tx, ty, im.s.h);
     const int w = im.s.w;
     if (r.x0 >= w) return;
     const bool full = r.x0 + P <= w;
-    for (int y = r.y; y < r.yend; y += 2 * r.step) {
-      const int y2 = y + r.step;
-      const bool two = y2 < r.yend;
-      const uint8_t *s0 = row_ptr<const uint8_t>(im.s, y) + (long long)r.x0 * SCN;
-      const uint8_t *s1 = row_ptr<const uint8_t>(im.s, two ? y2 : y) + (long long)r.x0 * SCN;
-      uint8_t *d0 = row_ptr<uint8_t>(im.d, y) + r.x0;
-      uint8_t *d1 = row_ptr<uint8_t>(im.d, two ? y2 : y) + r.x0;
-      if (full && (((uintptr_t)s0 | (uintptr_t)s1 | (uintptr_t)d0 | (uintptr_t)d1) % P) == 0) {
-        Vb<P, SCN> i0, i1;
-        i0.load(s0);
-        i1.load(s1);
-        Vb<P, 1> o0, o1;
-        px(i0, o0);
-        px(i1, o1);
-        o0.store(d0);
-        if (two) o1.store(d1);
+    for (int y = r.y; y < r.yend; y += U * r.step) {
+      const uint8_t *sp[U];
+      uint8_t *dp[U];
+      bool ok[U];
+      uintptr_t al = 0;
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int yy = y + u * r.step;
+        ok[u] = yy < r.yend;
+        const int ys = ok[u] ? yy : y;  // rows past the tile repeat row y (not stored)
+        sp[u] = row_ptr<const uint8_t>(im.s, ys) + (long long)r.x0 * SCN;
+        dp[u] = row_ptr<uint8_t>(im.d, ys) + r.x0;
+        al |= (uintptr_t)sp[u] | (uintptr_t)dp[u];
+      }
+      if (full && (al % P) == 0) {
+        Vb<P, SCN> in[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) in[u].load(sp[u]);
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+          Vb<P, 1> o;
+          px(in[u], o);
+          if (ok[u]) o.store(dp[u]);
+        }
       } else {
-        for (int i = 0; i < P && r.x0 + i < w; i++) {
-          d0[i] = (uint8_t)gray_px(s0[i * SCN], s0[i * SCN + 1], s0[i * SCN + 2]);
-          if (two) d1[i] = (uint8_t)gray_px(s1[i * SCN], s1[i * SCN + 1], s1[i * SCN + 2]);
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+          if (!ok[u]) break;
+          for (int i = 0; i < P && r.x0 + i < w; i++)
+            dp[u][i] = (uint8_t)gray_px(sp[u][i * SCN], sp[u][i * SCN + 1], sp[u][i * SCN + 2]);
         }
       }
     }
