@@ -160,6 +160,15 @@ def test_thresholds_warps_and_borders():
                       ("resize", {"fx": 0.5, "fy": 0.5, "interp": 3})])
 
 
+def test_every_strip_profile_fused_and_single():
+    """Each compiled element profile (rect 3/5/7, cross 3/5, ellipse 5/7) as
+    erode, dilate and the fused open / close, on 1-, 3- and 4-channel images."""
+    imgs = mixed_u8(6, seed=61, wmax=500, hmax=300, channels=(1, 3, 4))
+    for shape, k in ((0, 3), (0, 5), (0, 7), (1, 3), (1, 5), (2, 5), (2, 7)):
+        for op in (0, 1, 2, 3):
+            check_plan(imgs, [("morph", {"op": op, "shape": shape, "k": (k, k)})])
+
+
 def test_more_images_than_prefix_cache():
     rng = np.random.default_rng(21)
     imgs = []
