@@ -740,7 +740,7 @@ struct WarpArgs {
 // pixels (the per-call kernels' footprint).
 template <class T, int CN, bool PERSP>
 struct OpWarp {
-  static constexpr int kThreads = 256, TS = 32;
+  static constexpr int kThreads = 256, TS = 32, kMinBlocks = 4;  // <= 64 registers
   using Args = WarpArgs;
   static size_t smem(const Args &) { return 0; }
   static int tiles_x(int w) { return (int)ceil_div(w, TS); }
