@@ -111,6 +111,28 @@ def test_mixed_size_pipeline_matches_plain():
     check_plan(imgs, C2, graph=True, plan=plan)
 
 
+def test_mixed_batch_matches_oracle_directly():
+    """The C2 pipeline's final outputs against the CPU oracle itself (not only
+    through the per-call path), on a few uneven 1- and 3-channel images that
+    include odd sizes (general bilinear) and even ones (exact halving)."""
+    from oracle import oracle as O
+    shapes = [(67, 91, 3), (120, 200, 1), (53, 64, 3), (96, 130, 1), (201, 77, 3)]
+    imgs = [synth.base_image_torch(h, w, c, nrect=3, seed=700 + k) for k, (h, w, c) in enumerate(shapes)]
+    plan = B.Batch(imgs, [batch_stage(s) for s in C2])
+    plan.run_graph()
+    torch.cuda.synchronize()
+    for i, x in enumerate(imgs):
+        a = x.cpu().numpy()
+        y = a if a.ndim == 2 else O.cvt_color(a, 6)
+        y = O.gaussian_blur(y, (5, 5), 0, 0, 4)
+        y = O.morphology(y, 2, 2, (5, 5))
+        h, w = dims_after_resize(y.shape[0], y.shape[1], 0.5, 0.5)
+        if (h, w) != y.shape[:2]:
+            y = O.resize(y, (w, h), 1)
+        got = plan.output(i).cpu().numpy()
+        assert got.shape == y.shape and np.array_equal(got, y), i
+
+
 def test_video_frames_replayed_through_graph():
     h, w = 360, 640
     hom = synth.perspective_params(w, h, seed=7)
