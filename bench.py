@@ -39,6 +39,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -74,8 +75,7 @@ class Clocks:
     def __init__(self, gpu_index):
         self.gpu = gpu_index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else ".",
-                                 f".clocks_{os.getpid()}.csv")
+        self.path = os.path.join(tempfile.gettempdir(), f"visar_bench_clocks_{os.getpid()}_{id(self)}.csv")
 
     def __enter__(self):
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
@@ -124,6 +124,24 @@ class Clocks:
         if not sm:
             return None
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+_SYNTH = None
+
+
+def load_synth():
+    """visar_b200/synth.py loaded as a module of its own. The generators need
+    only NumPy (and torch for device images); loading the file directly keeps
+    the reference arm from importing the visar_b200 package, whose import maps
+    the CUDA library."""
+    global _SYNTH
+    if _SYNTH is None:
+        import importlib.util
+        spec = importlib.util.spec_from_file_location("visar_bench_synth", os.path.join(ROOT, "visar_b200", "synth.py"))
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        _SYNTH = mod
+    return _SYNTH
 
 
 def dist_setup(n):
@@ -197,7 +215,7 @@ MIX_SEED = 2
 
 
 def mixed_shapes():
-    from visar_b200 import synth
+    synth = load_synth()
     return synth.mixed_shapes(N_IMAGES, seed=MIX_SEED)
 
 
@@ -218,26 +236,76 @@ def c2_oracle_image(O, x):
     return y if (h, w) == y.shape[:2] else O.resize(y, (w, h), 1)
 
 
-def c2_cpu_sample(budget_s, max_images=N_IMAGES):
-    """Times the oracle on a bounded prefix of the batch (image generation untimed);
-    returns (Gpix/s, images, MP, s, threads)."""
+def oracle_run(fn, items, threads, budget_s, keep=False):
+    """Times fn(O, item) over items with the oracle on `threads` host threads
+    (0 = all) until the items or the time budget run out (one untimed call of
+    the first item first). Returns (items done, seconds, threads, outputs)."""
     from oracle import oracle as O
-    from visar_b200 import synth
-    O.set_num_threads(0)
-    shapes = mixed_shapes()
-    c2_oracle_image(O, synth.base_image(64, 64, 3, nrect=1, seed=0))  # warm-up
-    n = px = 0
-    dt = 0.0
-    for k, (h, w, c) in enumerate(shapes[:max_images]):
-        x = synth.base_image(h, w, c, nrect=8, seed=10_000 + k)
+    O.set_num_threads(threads)
+    fn(O, items[0])
+    outs = []
+    n, dt = 0, 0.0
+    oracle_run.times = []
+    for it in items:
         t0 = time.perf_counter()
-        c2_oracle_image(O, x)
-        dt += time.perf_counter() - t0
+        y = fn(O, it)
+        t1 = time.perf_counter() - t0
+        dt += t1
+        oracle_run.times.append(t1)
+        if keep:
+            outs.append(y)
         n += 1
-        px += h * w
         if dt > budget_s:
             break
-    return px / dt / 1e9, n, px / 1e6, dt, O.get_num_threads()
+    cores = O.get_num_threads()
+    O.set_num_threads(0)
+    return n, dt, cores, outs
+
+
+def cv2_c2_image(cv2, x):
+    """The C2 pipeline through OpenCV (context timing only: OpenCV 4's arithmetic
+    is not VISAR's everywhere)."""
+    y = x if x.ndim == 2 else cv2.cvtColor(x, cv2.COLOR_BGR2GRAY)
+    y = cv2.GaussianBlur(y, (5, 5), 0, borderType=cv2.BORDER_REFLECT_101)
+    y = cv2.morphologyEx(y, cv2.MORPH_OPEN, cv2.getStructuringElement(cv2.MORPH_ELLIPSE, (5, 5)))
+    h, w = half_dims(y.shape[0], y.shape[1])
+    return y if (h, w) == y.shape[:2] else cv2.resize(y, (w, h), interpolation=cv2.INTER_LINEAR)
+
+
+def cv2_context(fn, items, px_of, budget_s):
+    """OpenCV (all its threads) over a bounded prefix of items: Gpix/s, or None without cv2."""
+    try:
+        import cv2
+    except Exception:
+        return None
+    fn(cv2, items[0])
+    n, px, dt = 0, 0, 0.0
+    for it in items:
+        t0 = time.perf_counter()
+        fn(cv2, it)
+        dt += time.perf_counter() - t0
+        n += 1
+        px += px_of(it)
+        if dt > budget_s:
+            break
+    return {"value": px / dt / 1e9, "unit": "Gpix/s", "threads": cv2.getNumThreads(), "version": cv2.__version__,
+            "sample": f"{n} items, {px / 1e6:.1f} MP in {dt:.1f} s"}
+
+
+def c2_cpu_baselines(hosts, keep):
+    """The oracle on the C2 images: all host threads over the whole batch (its
+    outputs kept for the parity check when `keep`), then 1 thread and OpenCV
+    on bounded prefixes. Returns (cpu_baseline dict, outputs)."""
+    n, dt, cores, outs = oracle_run(c2_oracle_image, hosts, 0, 60.0, keep=keep)
+    px = sum(x.shape[0] * x.shape[1] for x in hosts[:n])
+    n1, dt1, _, _ = oracle_run(c2_oracle_image, hosts, 1, 15.0)
+    px1 = sum(x.shape[0] * x.shape[1] for x in hosts[:n1])
+    cpu = {"value": px / dt / 1e9, "unit": "Gpix/s", "cores": cores, "kind": "port",
+           "sample": f"{n} of the {len(hosts)} images ({px / 1e6:.1f} MP) through the 4-stage pipeline in {dt:.1f} s",
+           "one_thread": {"value": px1 / dt1 / 1e9, "unit": "Gpix/s", "cores": 1,
+                          "sample": f"first {n1} images ({px1 / 1e6:.1f} MP) in {dt1:.1f} s"},
+           "cv2_context": cv2_context(cv2_c2_image, hosts, lambda x: x.shape[0] * x.shape[1], 10.0)}
+    return cpu, outs
 
 
 def tune_workload(args, ctx, workload, images, stages, fill=None):
@@ -255,7 +323,7 @@ def tune_workload(args, ctx, workload, images, stages, fill=None):
 def bench_batched(args, ctx):
     torch, vb = ctx.torch, ctx.vb
     from visar_b200 import batch as B
-    from visar_b200 import synth
+    synth = load_synth()
     shapes = mixed_shapes()
     bases = [synth.base_image_torch(h, w, c, nrect=8, seed=10_000 + k) for k, (h, w, c) in enumerate(shapes)]
 
@@ -384,11 +452,17 @@ def bench_batched(args, ctx):
             raise AssertionError("downloaded output differs from the device result")
     del e_plans[1:]
 
-    cpu = None
+    # CPU baselines on the same images; the oracle's outputs for the whole
+    # batch are compared with the batched results (outside any timed region).
+    cpu, parity = None, None
     if ctx.rank == 0 and ctx.world == 1 and not args.no_cpu_baseline:
-        v, n, mp, dt, cores = c2_cpu_sample(10.0)
-        cpu = {"value": v, "unit": "Gpix/s", "cores": cores, "kind": "port",
-               "sample": f"first {n} of the {N_IMAGES} images ({mp:.1f} MP) through the 4-stage pipeline in {dt:.1f} s"}
+        host_in = [x.cpu().numpy() for x in ins]
+        cpu, ref_outs = c2_cpu_baselines(host_in, keep=True)
+        bad = [k for k, y in enumerate(ref_outs) if not np.array_equal(y, plan.output(k).cpu().numpy())]
+        parity = {"checked": len(ref_outs), "of": len(ins), "bit_exact": len(ref_outs) - len(bad),
+                  "summary": f"{len(ref_outs) - len(bad)}/{len(ins)} images bit-exact against the oracle",
+                  "first_mismatch": bad[0] if bad else None}
+        del host_in, ref_outs
     return {
         "metric": METRIC, "value": value, "unit": "Gpix/s", "n_gpus": ctx.world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
@@ -409,40 +483,39 @@ def bench_batched(args, ctx):
                      "traffic": load_traffic("batched-mixed", dom.split(":", 1)[1]),
                      "alg_bytes_per_launch": kernels[dom]["bytes"], "share_of_kernel_time": kernels[dom]["ms"] / all_ms},
         "cpu_baseline": cpu,
+        "parity": parity,
         "clocks": clocks,
         "gpu_launches": info["launches"] * args.steps,
     }
 
 
 def reference_batched(args):
-    """The oracle port on the host cores: each step a fixed bounded sample of the batch."""
+    """VISAR's CPU path (the oracle port) on all host threads: every step runs
+    the whole 256-image batch through the 4-stage pipeline, for the same warm-up
+    and step counts as the GPU arm."""
     from oracle import oracle as O
-    from visar_b200 import synth
+    synth = load_synth()
     O.set_num_threads(0)
     shapes = mixed_shapes()
-    sample, px = [], 0
-    for k, (h, w, c) in enumerate(shapes):  # about 25 MP per step
-        sample.append(synth.base_image(h, w, c, nrect=8, seed=10_000 + k))
-        px += h * w
-        if px >= 25e6:
-            break
-    for x in sample:
-        c2_oracle_image(O, x)
-    steps = max(1, min(args.steps, 10))
+    images = [synth.base_image(h, w, c, nrect=8, seed=10_000 + k) for k, (h, w, c) in enumerate(shapes)]
+    px = sum(h * w for (h, w, c) in shapes)
+    for _ in range(args.warmup):
+        for x in images:
+            c2_oracle_image(O, x)
     t0 = time.perf_counter()
-    for _ in range(steps):
-        for x in sample:
+    for _ in range(args.steps):
+        for x in images:
             c2_oracle_image(O, x)
     dt = time.perf_counter() - t0
-    v = px * steps / dt / 1e9
+    v = px * args.steps / dt / 1e9
     return {
-        "impl": "reference", "metric": METRIC, "value": v, "unit": "Gpix/s", "n_gpus": args.gpus, "steps": steps,
-        "warmup": args.warmup, "ms_per_step": dt / steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "Gpix/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u8", "data": "synthetic",
-        "config": {"workload": "batched-mixed", "images": N_IMAGES,
+        "config": {"workload": "batched-mixed", "images": N_IMAGES, "pixels_per_step": px,
                    "impl": "VISAR CPU path (C++ restatement, oracle/), all host threads"},
         "cpu_baseline": {"value": v, "unit": "Gpix/s", "cores": O.get_num_threads(), "kind": "port",
-                         "sample": f"first {len(sample)} images of the batch ({px / 1e6:.1f} MP) per step"},
+                         "sample": f"all {len(images)} images ({px / 1e6:.1f} MP) per step"},
         "e2e": {"value": v, "unit": "Gpix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -455,7 +528,7 @@ V_BYTES_PER_FRAME = V_W * V_H * 3 + V_W * V_H + 2 * V_W * V_H + 2 * V_W * V_H + 
 
 
 def video_homography():
-    from visar_b200 import synth
+    synth = load_synth()
     return synth.perspective_params(V_W, V_H, seed=7)
 
 
@@ -482,10 +555,19 @@ def video_oracle(O, x):
     return O.warp_perspective(y, video_homography(), (V_W, V_H), 1, 0, 0.0)
 
 
+def cv2_video_frame(cv2, x):
+    """The video pipeline through OpenCV (context timing only)."""
+    y = cv2.cvtColor(x, cv2.COLOR_BGR2GRAY)
+    y = cv2.GaussianBlur(y, (5, 5), 0, borderType=cv2.BORDER_REFLECT_101)
+    _, y = cv2.threshold(y, 100, 255, cv2.THRESH_BINARY)
+    y = cv2.morphologyEx(y, cv2.MORPH_CLOSE, cv2.getStructuringElement(cv2.MORPH_RECT, (7, 7)))
+    return cv2.warpPerspective(y, video_homography(), (V_W, V_H), flags=cv2.INTER_LINEAR, borderValue=0)
+
+
 def bench_video(args, ctx):
     torch, vb = ctx.torch, ctx.vb
     from visar_b200 import batch as B
-    from visar_b200 import synth
+    synth = load_synth()
     scene = synth.VideoScene(V_H, V_W, nobj=16, seed=3)
     frames = [scene.frame(k) for k in range(V_FRAMES)]  # 7.5 GB in HBM, outside timing
     torch.cuda.synchronize()
@@ -607,20 +689,28 @@ def bench_video(args, ctx):
     e_ms = ctx.max_over_ranks(e0.elapsed_time(e1)) / e_n
     vb.set_async(False)
 
-    cpu = None
+    # CPU baselines on the first frames; the oracle's results for those frames
+    # are compared with the graph's (outside any timed region).
+    cpu, parity = None, None
     if ctx.rank == 0 and ctx.world == 1 and not args.no_cpu_baseline:
-        from oracle import oracle as O
-        O.set_num_threads(0)
-        xs = [frames[k].cpu().numpy() for k in range(4)]
-        video_oracle(O, xs[0])
-        t0 = time.perf_counter()
-        n = 0
-        while time.perf_counter() - t0 < 8.0 and n < 20:
-            video_oracle(O, xs[n % 4])
-            n += 1
-        dt = time.perf_counter() - t0
-        cpu = {"value": n * V_W * V_H / dt / 1e9, "unit": "Gpix/s", "cores": O.get_num_threads(), "kind": "port",
-               "sample": f"{n} frames through the 5-stage pipeline in {dt:.1f} s ({n / dt:.2f} frames/s)"}
+        nchk = 4
+        xs = [frames[k].cpu().numpy() for k in range(8)]
+        n, dt, cores, ref = oracle_run(video_oracle, xs, 0, 8.0, keep=True)
+        n1, dt1, _, _ = oracle_run(video_oracle, xs, 1, 8.0)
+        cpu = {"value": n * V_W * V_H / dt / 1e9, "unit": "Gpix/s", "cores": cores, "kind": "port",
+               "sample": f"{n} frames through the 5-stage pipeline in {dt:.1f} s ({n / dt:.2f} frames/s)",
+               "one_thread": {"value": n1 * V_W * V_H / dt1 / 1e9, "unit": "Gpix/s", "cores": 1,
+                              "sample": f"{n1} frames in {dt1:.1f} s"},
+               "cv2_context": cv2_context(cv2_video_frame, xs, lambda x: V_W * V_H, 5.0)}
+        good = 0
+        for k in range(min(nchk, len(ref))):
+            plan.set_input(0, frames[k])
+            plan.run()
+            torch.cuda.synchronize()
+            good += bool(np.array_equal(plan.output(0).cpu().numpy(), ref[k]))
+        parity = {"checked": min(nchk, len(ref)), "bit_exact": good,
+                  "summary": f"{good}/{min(nchk, len(ref))} frames bit-exact against the oracle"}
+        del xs, ref
     return {
         "metric": METRIC, "value": value, "unit": "Gpix/s", "n_gpus": ctx.world, "steps": nf, "warmup": args.warmup,
         "ms_per_step": ms / nf, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
@@ -642,33 +732,35 @@ def bench_video(args, ctx):
                      "traffic": load_traffic("video-4k", dom.split(":", 1)[1]),
                      "alg_bytes_per_launch": kernels[dom]["bytes"]},
         "cpu_baseline": cpu,
+        "parity": parity,
         "clocks": clocks,
         "gpu_launches": (plan.info()["launches"] + 1) * nf,
     }
 
 
 def reference_video(args):
+    """The oracle port on all host threads: each step is one 4K frame through the
+    5-stage pipeline (frames rendered on the host, outside timing)."""
     from oracle import oracle as O
-    from visar_b200 import synth
-    import torch
+    synth = load_synth()
     O.set_num_threads(0)
     scene = synth.VideoScene(V_H, V_W, nobj=16, seed=3)
-    frames = [scene.frame(k, device="cpu").numpy() for k in range(3)]
-    video_oracle(O, frames[0])
-    steps = max(1, min(args.steps, 5))
+    frames = [scene.frame(k, device="cpu").numpy() for k in range(4)]
+    for k in range(args.warmup):
+        video_oracle(O, frames[k % 4])
     t0 = time.perf_counter()
-    for k in range(steps):
-        video_oracle(O, frames[k % 3])
+    for k in range(args.steps):
+        video_oracle(O, frames[k % 4])
     dt = time.perf_counter() - t0
-    v = steps * V_W * V_H / dt / 1e9
+    v = args.steps * V_W * V_H / dt / 1e9
     return {
-        "impl": "reference", "metric": METRIC, "value": v, "unit": "Gpix/s", "n_gpus": args.gpus, "steps": steps,
-        "warmup": args.warmup, "ms_per_step": dt / steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "Gpix/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u8", "data": "synthetic",
-        "config": {"workload": "video-4k", "frame": f"{V_W}x{V_H}x3 u8", "fps": steps / dt,
+        "config": {"workload": "video-4k", "frame": f"{V_W}x{V_H}x3 u8", "fps": args.steps / dt,
                    "impl": "VISAR CPU path (C++ restatement, oracle/), all host threads"},
         "cpu_baseline": {"value": v, "unit": "Gpix/s", "cores": O.get_num_threads(), "kind": "port",
-                         "sample": f"{steps} frames of the video pipeline"},
+                         "sample": f"{args.steps} frames of the video pipeline"},
         "e2e": {"value": v, "unit": "Gpix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -680,7 +772,7 @@ S_CORPUS = 384
 
 
 def served_stage_list(B, r):
-    from visar_b200 import synth
+    synth = load_synth()
     out = []
     for name, p in r["stages"]:
         if name == "gray":
@@ -696,12 +788,55 @@ def served_stage_list(B, r):
     return out
 
 
+def served_oracle(O, item):
+    """One served request's pipeline through module O (the oracle): gray is a
+    pass-through on one-channel images and the halving on 1-pixel sides, as
+    in the server."""
+    synth = load_synth()
+    r, x = item
+    for name, p in r["stages"]:
+        c = 1 if x.ndim == 2 else x.shape[2]
+        if name == "gray":
+            if c > 1:
+                x = O.cvt_color(x, 6 if c == 3 else 10)
+        elif name == "gauss":
+            x = O.gaussian_blur(x, (5, 5), 0, 0, 4)
+        elif name == "resize":
+            h, w = max(1, x.shape[0] // 2), max(1, x.shape[1] // 2)
+            if (h, w) != tuple(x.shape[:2]):
+                x = O.resize(x, (w, h), 1)
+        elif name == "affine":
+            m = synth.rotation_matrix_2d(r["w"] / 2.0, r["h"] / 2.0, p["angle"], 1.0)
+            x = O.warp_affine(x, m, (x.shape[1], x.shape[0]), 1, 0, 0.0)
+        else:
+            x = O.morphology(x, 2, 0, (3, 3))
+    return x
+
+
+def served_cpu_baseline(corpus, hosts, keep):
+    """The oracle over the corpus's requests in arrival order, one request at a
+    time on all host threads (VISAR's own per-call threading): Gpix/s of
+    request input pixels and the per-request service time (no queueing)."""
+    items = list(zip(corpus, hosts))
+    n, dt, cores, outs = oracle_run(served_oracle, items, 0, 15.0, keep=keep)
+    t = np.array(oracle_run.times) * 1e3
+    px = sum(r["h"] * r["w"] for r in corpus[:n])
+    n1, dt1, _, _ = oracle_run(served_oracle, items, 1, 10.0)
+    px1 = sum(r["h"] * r["w"] for r in corpus[:n1])
+    return {"value": px / dt / 1e9, "unit": "Gpix/s", "cores": cores, "kind": "port",
+            "sample": f"first {n} requests of the corpus ({px / 1e6:.1f} MP) one after another in {dt:.1f} s",
+            "service_p50_ms": float(np.percentile(t, 50)), "service_p99_ms": float(np.percentile(t, 99)),
+            "max_rate_req_s": n / dt,
+            "one_thread": {"value": px1 / dt1 / 1e9, "unit": "Gpix/s", "cores": 1,
+                           "sample": f"first {n1} requests in {dt1:.1f} s"}}, outs
+
+
 def bench_served(args, ctx):
     torch = ctx.torch
     import ctypes
     from visar_b200 import batch as B
     from visar_b200 import serve as S
-    from visar_b200 import synth
+    synth = load_synth()
     from visar_b200 import desc
     corpus = synth.served_requests(S_CORPUS, seed=4)
     imgs = [synth.served_image(r) for r in corpus]  # device-resident payloads
@@ -714,6 +849,7 @@ def bench_served(args, ctx):
     # (rate, requests): the spec rates for `dur` seconds each, then a
     # saturation run (every request queued at t = 0) that measures capacity.
     runs = [(rate, int(rate * dur)) for rate in S_RATES] + [(0, int(S_RATES[-1] * dur))]
+    clk = Clocks(ctx.dev).__enter__()  # sampled over every rate and both modes
     for rate, n in [(2000, 400)] + runs:  # the first run warms both modes up and is not reported
         if rate > 0:
             t = np.cumsum(rng.exponential(1.0 / rate, size=n))
@@ -752,7 +888,35 @@ def bench_served(args, ctx):
                 row["fallback_calls"] = st["fallback_calls"]
                 row["deferred"] = st["deferred"]
         results.append(row)
+    clk.__exit__(None, None, None)
+    clocks = clk.summary()
     results = results[1:]  # drop the warm-up run
+    cpu, parity = None, None
+    if ctx.rank == 0 and ctx.world == 1 and not args.no_cpu_baseline:
+        nchk = 96
+        hosts = [x.cpu().numpy() for x in imgs[:nchk]]
+        cpu, ref = served_cpu_baseline(corpus[:nchk], hosts, keep=True)
+        # The oracle's results against the server's for the same requests,
+        # all submitted at once so that they share launches.
+        srv = S.Server(pool_bytes=16 << 30)
+        try:
+            ids = [srv.submit(imgs[k], served_stage_list(B, corpus[k])) for k in range(len(ref))]
+            good = 0
+            for k, i in enumerate(ids):
+                y = srv.wait(i).cpu().numpy()
+                if corpus[k]["dtype"] == "u8":
+                    good += bool(y.shape == ref[k].shape and np.array_equal(y, ref[k]))
+                else:
+                    good += bool(y.shape == ref[k].shape and np.all(
+                        np.abs(y.astype(np.float64) - ref[k]) <= 1e-5 * np.maximum(1.0, np.abs(ref[k].astype(np.float64)))))
+                srv.release(i)
+            mb = srv.stats()["mean_batch"]
+        finally:
+            srv.close()
+        parity = {"checked": len(ref), "matching": good, "mean_batch": mb,
+                  "summary": f"{good}/{len(ref)} requests equal to the oracle (u8 bit-exact, f32 within 1e-5 relative), "
+                             f"served together"}
+        del hosts, ref
     sat = results[-1]
     sat["rate"] = "saturation"
     results = results[:-1]
@@ -771,15 +935,31 @@ def bench_served(args, ctx):
                                "p50/p99 per rate in per_rate; capacity in saturation"},
         "e2e": None,
         "roofline": None,
-        "cpu_baseline": None,
-        "clocks": None,
+        "cpu_baseline": cpu,
+        "parity": parity,
+        "clocks": clocks,
         "gpu_launches": int(sum(r["launches"] for r in results)),
     }
 
 
 def reference_served(args):
-    return {"impl": "reference", "unavailable": "served workload: VISAR has no request server; the oracle port "
-            "timings are in the batched-mixed reference line"}
+    """VISAR has no request server: its CPU path serves the corpus's requests
+    one after another on all host threads (images generated on the host)."""
+    synth = load_synth()
+    corpus = synth.served_requests(S_CORPUS, seed=4)[:96]
+    hosts = [synth.served_image(r, device="cpu").numpy() for r in corpus]
+    cpu, _ = served_cpu_baseline(corpus, hosts, keep=False)
+    v = cpu["value"]
+    return {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "Gpix/s", "n_gpus": args.gpus, "steps": 1,
+        "warmup": 1, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u8+f32", "data": "synthetic",
+        "config": {"workload": "served", "impl": "VISAR CPU path (C++ restatement, oracle/), one request at a time",
+                   "service_p50_ms": cpu["service_p50_ms"], "service_p99_ms": cpu["service_p99_ms"],
+                   "max_rate_req_s": cpu["max_rate_req_s"]},
+        "cpu_baseline": cpu,
+        "e2e": {"value": v, "unit": "Gpix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
 
 
 # ------------------------------------------------------------- plain-1080p
@@ -800,7 +980,7 @@ D2H_BYTES = sum(o[2] for o in OPS)
 
 
 def make_inputs():
-    from visar_b200 import synth
+    synth = load_synth()
     img = synth.base_image(H, W, 3, nrect=32, seed=1)
     f = synth.normal_f32(H, W, 1, seed=2)
     maff = synth.affine_params(W, H, seed=3)
@@ -842,20 +1022,34 @@ def alloc_outs(torch=None, pinned=False):
     return outs
 
 
-def plain_cpu_baseline(img, f, maff, mper, budget_s=12.0, max_steps=20):
-    """The oracle with all host threads, on a bounded sample."""
-    from oracle import oracle as O
-    O.set_num_threads(0)
+def plain_oracle_step(O, item):
+    img, f, maff, mper = item
     outs = alloc_outs()
-    run_step(O, img, f, maff, mper, outs)  # warm-up
-    t0 = time.perf_counter()
-    n = 0
-    while n < max_steps and (time.perf_counter() - t0) < budget_s:
-        run_step(O, img, f, maff, mper, outs)
-        n += 1
-    dt = time.perf_counter() - t0
-    return {"value": PIX_PER_STEP * n / dt / 1e9, "unit": "Gpix/s", "cores": O.get_num_threads(), "kind": "port",
-            "sample": f"{n} steps of the plain-1080p workload ({n * 5} calls, {PIX_PER_STEP * n / 1e6:.1f} MP) in {dt:.1f} s"}
+    run_step(O, img, f, maff, mper, outs)
+    return outs
+
+
+def cv2_plain_step(cv2, item):
+    """The plain-1080p calls through OpenCV (context timing only)."""
+    img, f, maff, mper = item
+    cv2.resize(img, (1280, 720), interpolation=cv2.INTER_LINEAR)
+    cv2.resize(img, (960, 540), interpolation=cv2.INTER_AREA)
+    cv2.warpAffine(img, maff, (W, H), flags=cv2.INTER_LINEAR, borderValue=0)
+    cv2.warpPerspective(img, mper, (W, H), flags=cv2.INTER_LINEAR, borderValue=0)
+    cv2.GaussianBlur(f, (7, 7), 1.5, borderType=cv2.BORDER_REFLECT_101)
+
+
+def plain_cpu_baseline(img, f, maff, mper, budget_s=12.0, max_steps=20):
+    """The oracle with all host threads (and with one) on a bounded number of
+    steps; returns (cpu_baseline, the oracle's outputs of one step)."""
+    items = [(img, f, maff, mper)] * max_steps
+    n, dt, cores, outs = oracle_run(plain_oracle_step, items, 0, budget_s, keep=True)
+    n1, dt1, _, _ = oracle_run(plain_oracle_step, items, 1, 6.0)
+    return ({"value": PIX_PER_STEP * n / dt / 1e9, "unit": "Gpix/s", "cores": cores, "kind": "port",
+             "sample": f"{n} steps of the plain-1080p workload ({n * 5} calls, {PIX_PER_STEP * n / 1e6:.1f} MP) in {dt:.1f} s",
+             "one_thread": {"value": PIX_PER_STEP * n1 / dt1 / 1e9, "unit": "Gpix/s", "cores": 1,
+                            "sample": f"{n1} steps in {dt1:.1f} s"},
+             "cv2_context": cv2_context(cv2_plain_step, items, lambda it: PIX_PER_STEP, 3.0)}, outs[0])
 
 
 def bench_plain(args, ctx):
@@ -903,9 +1097,20 @@ def bench_plain(args, ctx):
                                         before=lambda i: flush.fill_(i & 0xFF))) / args.steps
     e2e = PIX_PER_STEP * ctx.world / (e_ms / 1e3) / 1e9
     ctx.barrier()
-    cpu = None
+    cpu, parity = None, None
     if ctx.rank == 0 and ctx.world == 1 and not args.no_cpu_baseline:
-        cpu = plain_cpu_baseline(img, f, maff, mper)
+        cpu, ref = plain_cpu_baseline(img, f, maff, mper)
+        run_step(vb, d_img, d_f, maff, mper, d_outs)
+        torch.cuda.synchronize()
+        good = 0
+        for (name, _, _, _), y, r in zip(OPS, d_outs, ref):
+            y = y.cpu().numpy()
+            if y.dtype == np.float32:
+                good += bool(np.all(np.abs(y.astype(np.float64) - r) <= 1e-5 * np.maximum(1.0, np.abs(r.astype(np.float64)))))
+            else:
+                good += bool(np.array_equal(y, r))
+        parity = {"checked": len(OPS), "matching": good,
+                  "summary": f"{good}/{len(OPS)} calls equal to the oracle (u8 bit-exact, f32 within 1e-5 relative)"}
     return {
         "metric": METRIC, "value": value, "unit": "Gpix/s", "n_gpus": ctx.world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
@@ -920,6 +1125,7 @@ def bench_plain(args, ctx):
                      "frac": achieved / peak, "peak_kind": peak_kind, "traffic": load_traffic("plain-1080p", dom),
                      "alg_bytes_per_launch": ALG_BYTES[dom]},
         "cpu_baseline": cpu,
+        "parity": parity,
         "clocks": clocks,
         "gpu_launches": launches,
     }
@@ -930,22 +1136,141 @@ def reference_plain(args):
     O.set_num_threads(0)
     img, f, maff, mper = make_inputs()
     outs = alloc_outs()
-    for _ in range(max(1, min(args.warmup, 2))):
+    for _ in range(args.warmup):
         run_step(O, img, f, maff, mper, outs)
-    steps = max(1, min(args.steps, 10))
     t0 = time.perf_counter()
-    for _ in range(steps):
+    for _ in range(args.steps):
         run_step(O, img, f, maff, mper, outs)
     dt = time.perf_counter() - t0
-    v = PIX_PER_STEP * steps / dt / 1e9
+    v = PIX_PER_STEP * args.steps / dt / 1e9
     return {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "Gpix/s",
-        "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup, "ms_per_step": dt / steps * 1e3,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8+f32", "data": "synthetic",
         "config": {"workload": "plain-1080p", "frame": f"{W}x{H}x3 u8 + {W}x{H}x1 f32",
                    "ops": [o[0] for o in OPS], "impl": "VISAR CPU path (C++ restatement, oracle/), all host threads"},
         "cpu_baseline": {"value": v, "unit": "Gpix/s", "cores": O.get_num_threads(), "kind": "port",
-                         "sample": f"{steps} steps of plain-1080p"},
+                         "sample": f"{args.steps} steps of plain-1080p"},
+        "e2e": {"value": v, "unit": "Gpix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+# ------------------------------------------------------------------ c0-640
+
+C0_H, C0_W = 480, 640
+C0_NAMES = ["gray", "gaussian 5x5", "threshold 127", "erode 3x3 rect", "dilate 3x3 rect"]
+C0_BYTES = C0_H * C0_W * 3 + C0_H * C0_W + 4 * 2 * C0_H * C0_W  # in + out of each call
+
+
+def c0_pipeline(m, x, outs=None):
+    """The 640x480 pipeline through module m (the CUDA binding or the oracle);
+    returns every intermediate."""
+    o = outs or [None] * 5
+    g = m.cvt_color(x, 6, dst=o[0])
+    b = m.gaussian_blur(g, (5, 5), 0, 0, 4, dst=o[1])
+    t = m.threshold(b, 127, 255, 0, dst=o[2])
+    t = t[1] if isinstance(t, tuple) else t
+    e = m.morphology(t, 0, 0, (3, 3), 1, dst=o[3])
+    d = m.morphology(e, 1, 0, (3, 3), 1, dst=o[4])
+    return [g, b, t, e, d]
+
+
+def c0_input():
+    return load_synth().base_image(C0_H, C0_W, 3, nrect=8, seed=0)
+
+
+def bench_c0(args, ctx):
+    """The 640x480 BGR pipeline, call by call through the C ABI on device
+    images (value) and on host images (e2e), and as one batch plan replayed
+    as a CUDA graph (graph_us)."""
+    torch, vb = ctx.torch, ctx.vb
+    from visar_b200 import batch as B
+    x = c0_input()
+    d_x = torch.from_numpy(x).cuda()
+    d_outs = [torch.empty((C0_H, C0_W), dtype=torch.uint8, device="cuda") for _ in range(5)]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    vb.set_async(True)
+    steps = max(args.steps, 50)
+    for _ in range(args.warmup):
+        c0_pipeline(vb, d_x, d_outs)
+    ctx.barrier()
+    n0 = vb.launch_count()
+    with Clocks(ctx.dev) as clk:
+        ms = ctx.timed(lambda: c0_pipeline(vb, d_x, d_outs), steps, before=lambda i: flush.fill_(i & 0xFF))
+    launches = vb.launch_count() - n0
+    ctx.barrier()
+    ms_step = ctx.max_over_ranks(ms) / steps
+    clocks = clk.summary()
+    px = C0_H * C0_W
+    value = px * ctx.world / (ms_step / 1e3) / 1e9
+    # The same pipeline as a batch plan of one image, replayed as a graph.
+    plan = B.Batch([(C0_H, C0_W, 3, np.uint8)],
+                   [B.gray(), B.gaussian((5, 5), 0.0, 0.0, 4), B.threshold(127, 255, 0), B.morphology(0, 0, (3, 3), 1),
+                    B.morphology(1, 0, (3, 3), 1)])
+    plan.input(0).copy_(d_x)
+    for _ in range(args.warmup):
+        plan.run_graph()
+    g_ms = ctx.max_over_ranks(ctx.timed(plan.run_graph, steps, before=lambda i: flush.fill_(i & 0xFF))) / steps
+    vb.set_async(False)
+    # e2e: host images in pinned memory through the per-call C ABI.
+    h_x = torch.empty(x.shape, dtype=torch.uint8, pin_memory=True).numpy()
+    h_x[...] = x
+    h_outs = [torch.empty((C0_H, C0_W), dtype=torch.uint8, pin_memory=True).numpy() for _ in range(5)]
+    for _ in range(args.warmup):
+        c0_pipeline(vb, h_x, h_outs)
+    e_ms = ctx.max_over_ranks(ctx.timed(lambda: c0_pipeline(vb, h_x, h_outs), steps)) / steps
+    cpu, parity = None, None
+    if ctx.rank == 0 and ctx.world == 1 and not args.no_cpu_baseline:
+        items = [x] * 400
+        n, dt, cores, ref = oracle_run(lambda O, it: c0_pipeline(O, it), items, 0, 3.0, keep=True)
+        n1, dt1, _, _ = oracle_run(lambda O, it: c0_pipeline(O, it), items, 1, 3.0)
+        cpu = {"value": n * px / dt / 1e9, "unit": "Gpix/s", "cores": cores, "kind": "port",
+               "sample": f"{n} runs of the pipeline in {dt:.2f} s ({dt / n * 1e3:.3f} ms each)",
+               "one_thread": {"value": n1 * px / dt1 / 1e9, "unit": "Gpix/s", "cores": 1,
+                              "sample": f"{n1} runs in {dt1:.2f} s ({dt1 / n1 * 1e3:.3f} ms each)"}}
+        got = c0_pipeline(vb, d_x, d_outs)
+        torch.cuda.synchronize()
+        ok = [bool(np.array_equal(a.cpu().numpy(), b)) for a, b in zip(got, ref[0])]
+        ok_graph = bool(np.array_equal(plan.output(0).cpu().numpy(), ref[0][4]))
+        ok_host = [bool(np.array_equal(a, b)) for a, b in zip(h_outs, ref[0])]
+        parity = {"intermediates_bit_exact": dict(zip(C0_NAMES, ok)), "graph_bit_exact": ok_graph,
+                  "host_calls_bit_exact": all(ok_host),
+                  "summary": f"{sum(ok)}/5 intermediates bit-exact against the oracle"}
+    return {
+        "metric": METRIC, "value": value, "unit": "Gpix/s", "n_gpus": ctx.world, "steps": steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": "c0-640x480", "image": f"{C0_W}x{C0_H}x3 u8, seed 0, 8 rectangles", "stages": C0_NAMES,
+                   "latency_us": ms_step * 1e3, "graph_us": g_ms * 1e3, "graph_gpix_s": px / (g_ms / 1e3) / 1e9,
+                   "alg_bytes_per_step": C0_BYTES, "l2": "flushed before every timed step (256 MiB write)"},
+        "e2e": {"value": px * ctx.world / (e_ms / 1e3) / 1e9, "unit": "Gpix/s", "h2d_bytes_per_step": C0_BYTES // 2,
+                "d2h_bytes_per_step": 5 * px, "ms_per_step": e_ms},
+        "cpu_baseline": cpu,
+        "parity": parity,
+        "clocks": clocks,
+        "gpu_launches": launches,
+    }
+
+
+def reference_c0(args):
+    from oracle import oracle as O
+    O.set_num_threads(0)
+    x = c0_input()
+    steps = max(args.steps, 50)
+    for _ in range(args.warmup):
+        c0_pipeline(O, x)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        c0_pipeline(O, x)
+    dt = time.perf_counter() - t0
+    v = steps * C0_H * C0_W / dt / 1e9
+    return {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "Gpix/s", "n_gpus": args.gpus, "steps": steps,
+        "warmup": args.warmup, "ms_per_step": dt / steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": "c0-640x480", "impl": "VISAR CPU path (C++ restatement, oracle/), all host threads"},
+        "cpu_baseline": {"value": v, "unit": "Gpix/s", "cores": O.get_num_threads(), "kind": "port",
+                         "sample": f"{steps} runs of the pipeline"},
         "e2e": {"value": v, "unit": "Gpix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -953,7 +1278,16 @@ def reference_plain(args):
 # -------------------------------------------------------------------- main
 
 WORKLOADS = {"batched-mixed": (bench_batched, reference_batched), "plain-1080p": (bench_plain, reference_plain),
-             "video-4k": (bench_video, reference_video), "served": (bench_served, reference_served)}
+             "video-4k": (bench_video, reference_video), "served": (bench_served, reference_served),
+             "c0": (bench_c0, reference_c0)}
+# The other configs, reported as sub-objects of the batched-mixed line's
+# config when it runs on one GPU (the headline stays batched-mixed).
+SUBS = [("c0", "c0"), ("plain_1080p", "plain-1080p"), ("video_4k", "video-4k"), ("served", "served")]
+SUB_DROP = ("metric", "n_gpus", "higher_is_better", "scaling", "vs_baseline", "data")
+
+
+def sub_line(line):
+    return {k: v for k, v in line.items() if k not in SUB_DROP}
 
 
 def main():
@@ -963,20 +1297,36 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="batched-mixed", choices=sorted(WORKLOADS))
+    ap.add_argument("--only", action="store_true",
+                    help="batched-mixed alone (by default a 1-GPU run adds the other configs under config)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="built-in launch defaults instead of the tuned table")
     ap.add_argument("--tuning", default=None, help="tuned table to load, or to write when it was made elsewhere")
-    ap.add_argument("--duration", type=float, default=5.0, help="seconds per arrival rate (served workload)")
+    ap.add_argument("--duration", type=float, default=20.0, help="seconds per arrival rate (served workload)")
     args = ap.parse_args()
     ours, ref = WORKLOADS[args.workload]
+    subs = args.workload == "batched-mixed" and not args.only and args.gpus == 1
     if args.impl == "reference":
         if int(os.environ.get("RANK", "0")) != 0:
             return 0
-        print(json.dumps(ref(args)), flush=True)
+        line = ref(args)
+        if subs:
+            for key, wl in SUBS:
+                line["config"][key] = sub_line(WORKLOADS[wl][1](args))
+        print(json.dumps(line), flush=True)
         return 0
     args.warmup = max(3, args.warmup)
     ctx = Ctx(args)
     line = ours(args, ctx)
+    if subs and ctx.world == 1:
+        sub_args = argparse.Namespace(**vars(args))
+        sub_args.tuning = None
+        for key, wl in SUBS:
+            import gc
+            gc.collect()
+            ctx.torch.cuda.synchronize()
+            ctx.torch.cuda.empty_cache()
+            line["config"][key] = sub_line(WORKLOADS[wl][0](sub_args, ctx))
     ctx.barrier()
     if ctx.rank == 0:
         print(json.dumps(line), flush=True)

@@ -63,6 +63,17 @@ int visar_server_release(visar_server *s, uint64_t id);
 int visar_server_get_stats(visar_server *s, visar_server_stats *st);
 void visar_server_destroy(visar_server *s);
 
+/* Failure handling. When the completion check of a scheduling round returns
+   a CUDA error (the context's error is sticky, so the round's results and the
+   pool can no longer be trusted), every request that is not yet done
+   completes with VISAR_INTERNAL and the CUDA error's name
+   (visar_last_error), and every later submission fails the same way; the
+   server only has to be destroyed. visar_server_fake_round_error makes the
+   next completed round report `cuda_error` (a cudaError_t value) instead of
+   what the device said, so callers can test their handling of this path
+   without faulting a GPU. */
+int visar_server_fake_round_error(visar_server *s, int cuda_error);
+
 /* Load replay: submits n requests at their arrival times (seconds from the
    call, ascending) from a submitting thread, releases each result when it
    completes, and writes each request's latency (ms, submission to completion

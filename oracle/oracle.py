@@ -142,6 +142,15 @@ def threshold(a, thresh, maxval, kind, dst=None):
     return used.value, dst
 
 
+def resize_generic_u8(a, size, interpolation=1):
+    """VISAR's generic u8 kernels (linear: resize.zig:284-423; area:
+    areaGeneric), which its resize tests hold the dispatched fast paths to."""
+    w, h = size
+    dst = np.empty(_shape(a, w, h), np.uint8)
+    _check(lib.oracle_resize_generic_u8(ctypes.byref(desc(a)), ctypes.byref(desc(dst)), interpolation))
+    return dst
+
+
 def morphology(a, op, shape, ksize, iterations=1, dst=None):
     dst = np.empty_like(a) if dst is None else dst
     _check(lib.oracle_morphology(ctypes.byref(desc(a)), ctypes.byref(desc(dst)), op, shape, ksize[0], ksize[1], iterations))

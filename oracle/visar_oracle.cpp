@@ -17,6 +17,7 @@
 // Build: oracle/Makefile (g++ -O2 -ffp-contract=off: no fused multiply-adds
 // except where VISAR writes @mulAdd, which is std::fma here).
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <cmath>
 #include <cstdint>
@@ -936,6 +937,44 @@ void linear_u8(const Img<uint8_t> &s, const Img<uint8_t> &d, bool area) {
   });
 }
 
+// Generic `linear` (resize.zig:284-423) for u8: the definition VISAR tests its
+// u8 fast paths against (resize.zig:654-682). x taps from linearTapU8 (first
+// index and both weights); hrow sums s[xi]*a0 + s[xi+cn]*a1 in i32 (the second
+// tap is the first when xi is the row's last pixel); vrow rounds
+// ((r0 >> 4) * b0 >> 16) + ((r1 >> 4) * b1 >> 16), then (+2) >> 2, saturated.
+void linear_generic_u8(const Img<uint8_t> &s, const Img<uint8_t> &d, bool area) {
+  const int cn = s.cn;
+  const size_t n = d.row_len();
+  std::vector<uint32_t> xofs(n);
+  std::vector<std::array<int, 2>> alpha(n);
+  for (int x = 0; x < d.w; x++) {
+    const Tap2 t = linear_tap_u8(x, s.w, d.w, area, true);
+    for (int c = 0; c < cn; c++) {
+      xofs[(size_t)x * cn + c] = (uint32_t)t.o[0] * cn + c;
+      alpha[(size_t)x * cn + c] = {t.w[0], t.w[1]};
+    }
+  }
+  const size_t last_x = s.row_len() - cn;
+  std::vector<int32_t> r0(n), r1(n);
+  auto hrow = [&](const uint8_t *row, int32_t *out) {
+    for (size_t i = 0; i < n; i++) {
+      const size_t xi = xofs[i];
+      const size_t x1 = xi >= last_x ? xi : xi + cn;
+      out[i] = (int32_t)row[xi] * alpha[i][0] + (int32_t)row[x1] * alpha[i][1];
+    }
+  };
+  for (int y = 0; y < d.h; y++) {
+    const Tap2 t = linear_tap_u8(y, s.h, d.h, area, false);
+    hrow(s.row(t.o[0]), r0.data());
+    hrow(s.row(t.o[1]), r1.data());
+    uint8_t *o = d.row(y);
+    for (size_t i = 0; i < n; i++) {
+      const int32_t v = (((r0[i] >> 4) * t.w[0]) >> 16) + (((r1[i] >> 4) * t.w[1]) >> 16);
+      o[i] = cast<uint8_t>((v + 2) >> 2);
+    }
+  }
+}
+
 // ru8.half (resize_u8.zig:384-447).
 void half_u8(const Img<uint8_t> &s, const Img<uint8_t> &d) {
   const int cn = s.cn;
@@ -1772,6 +1811,19 @@ int oracle_resize(const visar_image *src, const visar_image *dst, int interp) {
     if (interp < 0 || interp > 4) fail(VISAR_UNSUPPORTED, "Unsupported");
     const int depth = src_depth(src);
     ORACLE_DISPATCH(depth, resize_d, src, dst, depth, interp);
+  });
+}
+
+// The generic kernels VISAR's resize tests compare its dispatch against
+// (resize.zig:654-682 `linear`, :701-743 `areaGeneric`); u8 only.
+int oracle_resize_generic_u8(const visar_image *src, const visar_image *dst, int interp) {
+  return guarded([&] {
+    Img<uint8_t> s = typed<uint8_t>(src, 0);
+    Img<uint8_t> d = typed<uint8_t>(dst, 0);
+    if (s.cn != d.cn) fail(VISAR_SIZE_MISMATCH, "SizeMismatch");
+    if (interp == 1) linear_generic_u8(s, d, false);
+    else if (interp == 3) area_generic(s, d);
+    else fail(VISAR_UNSUPPORTED, "Unsupported");
   });
 }
 

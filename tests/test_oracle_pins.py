@@ -173,3 +173,165 @@ def test_threads_do_not_change_results(threads):
     O.set_num_threads(0)
     for x, y in zip(ref, got):
         assert np.array_equal(x, y)
+
+
+# ------------------------------------------------------------ resize property tests
+# VISAR's own resize tests (resize.zig:642-743), on the oracle; the same cases
+# run through the CUDA library in test_pins_gpu.py.
+
+import pins_resize as PR  # noqa: E402
+
+
+@pytest.mark.parametrize("cn", [1, 2, 3, 4])
+def test_u8_linear_dispatch_equals_generic_kernel(cn):
+    # resize.zig:654-682: the dispatched u8 INTER_LINEAR (exact half, exact 2x,
+    # fast paths) equals the generic fixed-point `linear` kernel.
+    src = PR.lcg_image(150, 64, cn, 12345)
+    for w, h in PR.LINEAR_SIZES:
+        assert np.array_equal(O.resize(src, (w, h), 1), O.resize_generic_u8(src, (w, h), 1)), (cn, w, h)
+
+
+def test_resize_constant_stays_constant():
+    # resize.zig:642-652: 10x10x3 of 100 -> 7x13 under every interpolation.
+    src = np.full((10, 10, 3), 100, np.uint8)
+    for interp in (0, 1, 3, 2):
+        assert (O.resize(src, (7, 13), interp) == 100).all(), interp
+
+
+@pytest.mark.parametrize("cn", [1, 2, 3, 4])
+def test_nearest_equals_naive_mapping(cn):
+    # resize.zig:684-700
+    src = PR.hash_image(37, 11, cn)
+    for w, h in PR.NEAREST_SIZES:
+        assert np.array_equal(O.resize(src, (w, h), 0), PR.nearest_naive(src, w, h)), (cn, w, h)
+
+
+@pytest.mark.parametrize("cn", [1, 2, 3, 4])
+def test_area_dispatch_equals_generic_and_integer_rounding(cn):
+    # resize.zig:702-743: the dispatched u8 INTER_AREA equals areaGeneric, and
+    # 4x3 / 4x4 integer factors equal the f32 block-sum rounding.
+    src = PR.lcg_image(97, 61, cn, 777)
+    for w, h in PR.AREA_SIZES:
+        assert np.array_equal(O.resize(src, (w, h), 3), O.resize_generic_u8(src, (w, h), 3)), (cn, w, h)
+    s2 = np.ascontiguousarray(src[:60, :96])
+    for fx, fy in [(4, 3), (4, 4)]:
+        assert np.array_equal(O.resize(s2, (96 // fx, 60 // fy), 3), PR.area_int_naive(s2, fx, fy)), (cn, fx, fy)
+
+
+# ---------------------------------------------------- linear / cubic against cv2 4.13
+
+SHAPES = [(480, 640), (37, 53), (64, 150), (1, 9), (7, 1), (61, 97)]
+
+
+def _dsizes(h, w):
+    out = [(max(1, w * 3 // 4), max(1, h * 2 // 3)), (113, 71), (w * 2, h * 2), (75, 32)]
+    return [d for d in out if d != (w, h)]
+
+
+@pytest.mark.parametrize("h,w", SHAPES)
+def test_generic_linear_f32_u16_pinned(h, w):
+    # The NumPy restatement of the generic kernel (resize.zig:284-423) equals
+    # the oracle bit for bit; given OpenCV 4's f32 source coordinates instead
+    # of VISAR's f64 ones it equals cv2 4.13's portable build bit for bit, so
+    # VISAR and OpenCV 4 differ only in that step. (Exact halvings are left out
+    # of the cv2 side: OpenCV 4 runs them through INTER_AREA.)
+    import cv2
+    opt = cv2.useOptimized()
+    cv2.setUseOptimized(False)
+    try:
+        for cn in (1, 2, 3, 4):
+            for dt in (np.float32, np.uint16):
+                a = natural(h, w, cn, dt)
+                for dw, dh in _dsizes(h, w) + [(max(1, w // 2), max(1, h // 2))]:
+                    ours = O.resize(a, (dw, dh), 1)
+                    assert np.array_equal(ours, PR.linear_generic(a, dw, dh)), (cn, dt, dw, dh)
+                    if (dw * 2, dh * 2) != (w, h):
+                        ref = cv2.resize(a, (dw, dh), interpolation=cv2.INTER_LINEAR).reshape(ours.shape)
+                        assert np.array_equal(PR.linear_generic(a, dw, dh, opencv4=True), ref), (cn, dt, dw, dh)
+    finally:
+        cv2.setUseOptimized(opt)
+
+
+@pytest.mark.parametrize("h,w", SHAPES)
+def test_u8_linear_equals_cv2(h, w):
+    # u8 INTER_LINEAR (linearU8 / half / up2Linear) equals cv2 4.13 exactly,
+    # except 2-channel exact halvings, which OpenCV 4 sends through its area path.
+    import cv2
+    for cn in (1, 2, 3, 4):
+        a = natural(h, w, cn)
+        for dw, dh in _dsizes(h, w) + [(max(1, w // 2), max(1, h // 2))]:
+            if cn == 2 and (dw * 2, dh * 2) == (w, h):
+                continue
+            ours = O.resize(a, (dw, dh), 1)
+            assert np.array_equal(ours, cv2.resize(a, (dw, dh), interpolation=1).reshape(ours.shape)), (cn, dw, dh)
+
+
+@pytest.mark.parametrize("h,w", SHAPES)
+def test_cubic_u8_pinned(h, w):
+    # cubicU8 / up2Cubic: the NumPy restatement (taps, integer horizontal
+    # pass, vcubic's fused f32 chain) equals the oracle bit for bit; with
+    # OpenCV's unfused chain and integer row tail it equals cv2 4.13's portable
+    # build bit for bit. Taps, offsets and horizontal sums are therefore
+    # OpenCV's; only the fusing of the vertical chain differs.
+    import cv2
+    opt = cv2.useOptimized()
+    cv2.setUseOptimized(False)
+    try:
+        for cn in (1, 2, 3, 4):
+            a = natural(h, w, cn)
+            for dw, dh in _dsizes(h, w) + [(max(1, w // 2), max(1, h // 2))]:
+                ours = O.resize(a, (dw, dh), 2)
+                assert np.array_equal(ours, PR.cubic_u8(a, dw, dh, "visar")), (cn, dw, dh)
+                ref = cv2.resize(a, (dw, dh), interpolation=cv2.INTER_CUBIC).reshape(ours.shape)
+                assert np.array_equal(PR.cubic_u8(a, dw, dh, "opencv4"), ref), (cn, dw, dh)
+    finally:
+        cv2.setUseOptimized(opt)
+
+
+# ------------------------------------------------------------------ warp known answers
+
+def test_warp_known_answers():
+    import pins_warp
+    bad = pins_warp.check_all(O)
+    assert not bad, bad[:10]
+
+
+# ----------------------------------------------------------------- sepFilter2D vs cv2
+
+def _sep_cases():
+    ints = [([1, -2, 1], [1, 2, 1]), ([1, 4, 6, 4, 1], [-1, 0, 1]), ([3], [1, 1, 1, 1, 1, 1, 1]), ([2, -1, 0, 5, 1], [1, 3, -2])]
+    floats = [([0.1, 0.25, 0.3, 0.25, 0.1], [0.2, 0.6, 0.2]), ([-0.5, 0.0, 1.5], [0.7]), ([1.0 / 3] * 3, [0.05, 0.9, 0.05, 0.3, -0.1])]
+    return ints, floats
+
+
+@pytest.mark.parametrize("h,w", [(37, 53), (1, 9), (7, 1), (64, 150)])
+def test_sep_filter_2d_against_cv2(h, w):
+    # filter.zig:909-914 has no VISAR test. Integer taps on u8: every f32 sum
+    # is an exact integer, so VISAR's vertical-first and OpenCV's
+    # horizontal-first orders must agree exactly (saturated); f32 images agree
+    # within the 1e-5 contract.
+    import cv2
+    ints, floats = _sep_cases()
+    for cn in (1, 3):
+        u8 = natural(h, w, cn)
+        f = natural(h, w, cn, np.float32)
+        for border in (0, 1, 2, 4):
+            for kx, ky in ints:
+                ours = O.sep_filter_2d(u8, np.uint8, kx, ky, border)
+                ref = cv2.sepFilter2D(u8, -1, np.float32(kx), np.float32(ky), borderType=border).reshape(ours.shape)
+                assert np.array_equal(ours, ref), (cn, border, kx, ky)
+            for kx, ky in ints + floats:
+                ours = O.sep_filter_2d(f, np.float32, kx, ky, border).astype(np.float64)
+                assert ours.shape[:2] == (h, w)
+                ref = cv2.sepFilter2D(f, -1, np.float32(kx), np.float32(ky), borderType=border).reshape(ours.shape)
+                err = np.abs(ours - ref) / np.maximum(1.0, np.abs(ref))
+                assert err.max() <= 1e-5, (cn, border, kx, ky, err.max())
+
+
+def test_sep_filter_2d_even_kernels_refused():
+    # filter.zig:122: kernels of even length are InvalidKernel.
+    a = natural(9, 11, 1)
+    for kx, ky in [([1, 1], [1]), ([1], [1, 2, 1, 0])]:
+        with pytest.raises(O.OracleError) as e:
+            O.sep_filter_2d(a, np.uint8, kx, ky, 4)
+        assert e.value.status == -1 and "InvalidKernel" in e.value.name

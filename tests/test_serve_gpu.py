@@ -98,7 +98,7 @@ def test_results_match_per_call_pipeline():
 def test_same_result_alone_and_in_a_mix():
     reqs = small_requests(60, seed=12)
     imgs = [synth.served_image(r) for r in reqs]
-    probe = [k for k, r in enumerate(reqs) if len(r["stages"]) >= 2][:3]
+    probe = list(range(len(reqs)))
     srv = S.Server(pool_bytes=2 << 30)
     try:
         alone = {}
@@ -165,3 +165,38 @@ def test_trace_replay_completes():
             assert st["completed"] == len(reqs) and st["released"] == len(reqs) and st["pool_used"] == 0
         finally:
             srv.close()
+
+
+def test_device_error_fails_requests_and_later_submissions():
+    # A completion check that returns a CUDA error (faked here: no GPU fault
+    # is raised) fails every request not yet done with Internal and the
+    # error's name, and every later submission the same way.
+    reqs = small_requests(12, seed=16)
+    imgs = [synth.served_image(r) for r in reqs]
+    srv = S.Server(pool_bytes=1 << 30)
+    try:
+        srv.fake_round_error(700)  # cudaErrorIllegalAddress
+        ids = [srv.submit(x, stage_list(r)) for r, x in zip(reqs, imgs)]
+        failed = 0
+        for i in ids:
+            try:
+                srv.wait(i)
+            except vb.VisarError as e:
+                assert e.status == -6 and "cudaErrorIllegalAddress" in e.name
+                failed += 1
+        assert failed >= 1
+        late = srv.submit(imgs[0], stage_list(reqs[0]))
+        with pytest.raises(vb.VisarError) as e:
+            srv.wait(late)
+        assert e.value.status == -6 and "cudaErrorIllegalAddress" in e.value.name
+    finally:
+        srv.close()
+    # A new server on the same device is unaffected.
+    srv = S.Server(pool_bytes=1 << 30)
+    try:
+        i = srv.submit(imgs[0], stage_list(reqs[0]))
+        y = srv.wait(i).clone()
+        srv.release(i)
+        check(reqs[:1], imgs[:1], [y])
+    finally:
+        srv.close()

@@ -234,6 +234,8 @@ struct visar_server {
   uint64_t next_id = 1;
   size_t reserved = 0;
   std::atomic<bool> stop{false};
+  std::string broken;  // set once a device error was seen: the server only fails requests from then on
+  std::atomic<int> fake_round_error{0};  // visar_server_fake_round_error: the next completed round reports it
   std::thread worker;
   visar_server_stats stats{};
   uint64_t groups = 0, grouped = 0;
@@ -297,6 +299,37 @@ struct visar_server {
     }
   }
 
+  // A device error was seen (mu held). The context's error is sticky, so no
+  // later round can be trusted: every request not yet done completes now
+  // with Internal and the CUDA error's name, the rounds in flight are
+  // dropped without returning their blocks to the pool, and from here on
+  // new submissions fail the same way.
+  void fail_all(cudaError_t e) {
+    if (broken.empty()) broken = std::string("Internal: ") + cudaGetErrorName(e);
+    std::vector<uint64_t> ids;
+    for (auto &kv : reqs)
+      if (kv.second->state < 2) ids.push_back(kv.first);
+    const double t = now_s();
+    for (uint64_t id : ids) {
+      auto it = reqs.find(id);
+      if (it == reqs.end()) continue;
+      Req &q = *it->second;
+      q.status = VISAR_INTERNAL;
+      q.error = broken;
+      q.ready = nullptr;
+      q.next = (int)q.st.size();
+      finished(id, t);
+    }
+    for (Round &r : rounds) {
+      free_events.push_back(r.ev_launch);
+      free_events.push_back(r.ev_fb);
+    }
+    rounds.clear();
+    incoming.clear();
+    admitted.clear();
+    cv_done.notify_all();
+  }
+
   // Moves new submissions into the request table (takes mu_in; mu held).
   void take_pending() {
     std::vector<std::unique_ptr<Req>> got;
@@ -315,11 +348,22 @@ struct visar_server {
   void poll_rounds() {
     while (!rounds.empty()) {
       Round &r = rounds.front();
-      if (cudaEventQuery(r.ev_launch) == cudaErrorNotReady || cudaEventQuery(r.ev_fb) == cudaErrorNotReady) {
+      cudaError_t e1 = cudaEventQuery(r.ev_launch);
+      const cudaError_t e2 = e1 == cudaSuccess ? cudaEventQuery(r.ev_fb) : e1;
+      if (e1 == cudaErrorNotReady || e2 == cudaErrorNotReady) {
         cudaGetLastError();
         break;
       }
-      cudaGetLastError();
+      if (const int f = fake_round_error.exchange(0)) e1 = static_cast<cudaError_t>(f);
+      if (e1 != cudaSuccess || e2 != cudaSuccess) {
+        // A device error is sticky: the round's outputs are undefined and the
+        // pool may hold garbage. Fail every request of the round and every
+        // request still in flight, and stop admitting work.
+        const cudaError_t e = e1 != cudaSuccess ? e1 : e2;
+        cudaGetLastError();
+        fail_all(e);
+        return;
+      }
       for (void *p : r.blocks) pool.free(p);
       if (r.staging) staging.release(r.staging, r.staging_end);
       const double t = now_s();
@@ -619,9 +663,10 @@ struct visar_server {
       {
         std::lock_guard<std::mutex> lk(mu);
         take_pending();
+        if (!broken.empty() && !incoming.empty()) fail_all(cudaSuccess);
         poll_rounds();
         admit();
-        if ((int)rounds.size() < cfg.max_inflight)
+        if (broken.empty() && (int)rounds.size() < cfg.max_inflight)
           did = cfg.mode == VISAR_SERVE_PLAIN ? launch_plain() : launch_round();
       }
       if (!did) std::this_thread::sleep_for(std::chrono::microseconds(20));
@@ -755,6 +800,12 @@ int visar_server_release(visar_server *s, uint64_t id) {
   if (it == s->reqs.end() || it->second->state != 2 || it->second->trace)
     return report_error(VISAR_INVALID_ARGUMENT, "InvalidArgument: request not done");
   s->release_locked(it);
+  return VISAR_OK;
+}
+
+int visar_server_fake_round_error(visar_server *s, int cuda_error) {
+  if (!s || cuda_error <= 0) return report_error(VISAR_INVALID_ARGUMENT, "InvalidArgument");
+  s->fake_round_error.store(cuda_error);
   return VISAR_OK;
 }
 

@@ -43,6 +43,7 @@ lib.visar_server_release.argtypes = [ctypes.c_void_p, ctypes.c_uint64]
 lib.visar_server_get_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(ServerStats)]
 lib.visar_server_destroy.argtypes = [ctypes.c_void_p]
 lib.visar_server_destroy.restype = None
+lib.visar_server_fake_round_error.argtypes = [ctypes.c_void_p, ctypes.c_int]
 lib.visar_server_run_trace.argtypes = [ctypes.c_void_p, ctypes.POINTER(TraceRequest), ctypes.c_size_t,
                                        ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
 
@@ -105,6 +106,11 @@ class Server:
         st = ServerStats()
         _check(lib.visar_server_get_stats(self._h, ctypes.byref(st)))
         return {k: getattr(st, k) for k, _ in ServerStats._fields_}
+
+    def fake_round_error(self, cuda_error):
+        """The next completed scheduling round reports `cuda_error` (a
+        cudaError_t value) as if the device had raised it (failure-path tests)."""
+        _check(lib.visar_server_fake_round_error(self._h, int(cuda_error)))
 
     def run_trace(self, trace):
         """trace: list of (arrival_s, tensor, stages). Returns (latency_ms array, elapsed_s)."""
