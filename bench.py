@@ -1275,18 +1275,120 @@ def reference_c0(args):
     }
 
 
+# ------------------------------------------------------ next rows (f1-f3)
+
+N_W, N_H = 3840, 2160
+
+
+def timed_op(ctx, fn, n, flush):
+    """Mean ms of fn over n launches, L2 flushed (256 MiB write) before each."""
+    for _ in range(3):
+        fn()
+    return ctx.timed(fn, n, before=lambda i: flush.fill_(i & 0xFF)) / n
+
+
+def bench_next(args, ctx):
+    """The rows after the core path: fused gray + integer shrink
+    (visar_gray_downsample) on 4K BGR / BGRA frames, pyrDown / pyrUp on 4K,
+    undistort and remap on 1080p BGR. Per call: device-image time (CUDA
+    events, L2 flushed), algorithmic GB/s against the HBM peak, the oracle on
+    the host cores, and the results against the oracle."""
+    torch, vb = ctx.torch, ctx.vb
+    from oracle import oracle as O
+    synth = load_synth()
+    peak, peak_kind = load_peaks()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    n = max(10, args.steps)
+    cpu_ok = ctx.rank == 0 and ctx.world == 1 and not args.no_cpu_baseline
+    out = {}
+    vb.set_async(True)
+
+    def row(name, fn, nbytes, px, oracle_fn=None, got=None, cpu_items=None):
+        ms = ctx.max_over_ranks(timed_op(ctx, fn, n, flush))
+        r = {"ms": ms, "gpix_s": px / (ms / 1e3) / 1e9, "alg_bytes": nbytes, "gbs": nbytes / (ms / 1e3) / 1e9,
+             "frac": nbytes / (ms / 1e3) / 1e9 / peak}
+        if cpu_ok and oracle_fn is not None:
+            nn, dt, cores, ref = oracle_run(lambda O_, it: oracle_fn(), [0] * 20, 0, 3.0, keep=True)
+            n1, dt1, _, _ = oracle_run(lambda O_, it: oracle_fn(), [0] * 4, 1, 3.0)
+            r["cpu_baseline"] = {"value": nn * px / dt / 1e9, "unit": "Gpix/s", "cores": cores, "kind": "port",
+                                 "one_thread_gpix_s": n1 * px / dt1 / 1e9}
+            g = got()
+            r["bit_exact_vs_oracle"] = bool(np.array_equal(g, ref[0]))
+        return r
+
+    # f1: gray + integer shrink
+    for cn in (3, 4):
+        img = synth.base_image(N_H, N_W, cn, nrect=32, seed=20 + cn)
+        d_img = torch.from_numpy(img).cuda()
+        for k in (2, 3, 4, 8, 16):
+            dst = torch.empty((N_H // k, N_W // k), dtype=torch.uint8, device="cuda")
+            nbytes = N_W * N_H * cn + (N_W // k) * (N_H // k)
+            out[f"gray_downsample.c{cn}.k{k}"] = row(
+                f"gd{cn}{k}", lambda: vb.gray_downsample(d_img, k, dst=dst), nbytes, N_W * N_H,
+                oracle_fn=lambda: O.gray_downsample(img, k), got=lambda: dst.cpu().numpy())
+        # e2e: pinned host frame in, result out, through the C ABI
+        torch.cuda.synchronize()
+        h_img = torch.empty(img.shape, dtype=torch.uint8, pin_memory=True).numpy()
+        h_img[...] = img
+        h_dst = torch.empty((N_H // 2, N_W // 2), dtype=torch.uint8, pin_memory=True).numpy()
+        e_ms = ctx.timed(lambda: vb.gray_downsample(h_img, 2, dst=h_dst), n) / n
+        out[f"gray_downsample.c{cn}.k2"]["e2e_gpix_s"] = N_W * N_H / (e_ms / 1e3) / 1e9
+    # f2: pyramids
+    img = synth.base_image(N_H, N_W, 3, nrect=32, seed=31)
+    d_img = torch.from_numpy(img).cuda()
+    dd = torch.empty((N_H // 2, N_W // 2, 3), dtype=torch.uint8, device="cuda")
+    out["pyr_down.u8.c3.4k"] = row("pd", lambda: vb.pyr_down(d_img, 4, dst=dd), N_W * N_H * 3 * 5 // 4, N_W * N_H,
+                                   oracle_fn=lambda: O.pyr_down(img, 4), got=lambda: dd.cpu().numpy())
+    half = np.ascontiguousarray(img[::2, ::2])
+    d_half = torch.from_numpy(half).cuda()
+    du = torch.empty((N_H, N_W, 3), dtype=torch.uint8, device="cuda")
+    out["pyr_up.u8.c3.to4k"] = row("pu", lambda: vb.pyr_up(d_half, 4, dst=du), N_W * N_H * 3 * 5 // 4, N_W * N_H // 4,
+                                   oracle_fn=lambda: O.pyr_up(half, 4), got=lambda: du.cpu().numpy())
+    f = synth.normal_f32(N_H, N_W, 1, seed=32)
+    d_f = torch.from_numpy(f).cuda()
+    dfd = torch.empty((N_H // 2, N_W // 2), dtype=torch.float32, device="cuda")
+    out["pyr_down.f32.c1.4k"] = row("pdf", lambda: vb.pyr_down(d_f, 4, dst=dfd), N_W * N_H * 4 * 5 // 4, N_W * N_H,
+                                    oracle_fn=lambda: O.pyr_down(f, 4), got=lambda: dfd.cpu().numpy())
+    # f3: undistort / maps / remap on 1080p BGR
+    W1, H1 = 1920, 1080
+    img = synth.base_image(H1, W1, 3, nrect=32, seed=33)
+    d_img = torch.from_numpy(img).cuda()
+    K = np.array([[1000.0, 0, 959.5], [0, 1000.0, 539.5], [0, 0, 1]])
+    dist = [-0.28, 0.09, 0.0008, -0.0004, -0.012]
+    du = torch.empty_like(d_img)
+    out["undistort.u8.c3.1080p"] = row("ud", lambda: vb.undistort(d_img, K, dist, None, dst=du), 2 * W1 * H1 * 3, W1 * H1,
+                                       oracle_fn=lambda: O.undistort(img, K, dist), got=lambda: du.cpu().numpy())
+    mx = torch.empty((H1, W1), dtype=torch.float32, device="cuda")
+    my = torch.empty((H1, W1), dtype=torch.float32, device="cuda")
+    out["init_undistort_map.1080p"] = row(
+        "um", lambda: vb.init_undistort_rectify_map(K, dist, None, None, (W1, H1), mapx=mx, mapy=my), 8 * W1 * H1, W1 * H1,
+        oracle_fn=lambda: O.init_undistort_rectify_map(K, dist, None, None, (W1, H1))[0], got=lambda: mx.cpu().numpy())
+    dr = torch.empty_like(d_img)
+    hmx, hmy = mx.cpu().numpy(), my.cpu().numpy()
+    out["remap.u8.c3.1080p"] = row("rm", lambda: vb.remap(d_img, mx, my, 0.0, dst=dr), 2 * W1 * H1 * 3 + 8 * W1 * H1, W1 * H1,
+                                   oracle_fn=lambda: O.remap(img, hmx, hmy, 0.0), got=lambda: dr.cpu().numpy())
+    torch.cuda.synchronize()
+    vb.set_async(False)
+    return {"workload": "next-rows", "peak_gbs": peak, "peak_kind": peak_kind,
+            "timing": "device images, CUDA events, L2 flushed (256 MiB write) before each launch",
+            "alg_bytes": "source + destination bytes once (remap adds its two f32 maps)", "calls": out}
+
+
 # -------------------------------------------------------------------- main
 
 WORKLOADS = {"batched-mixed": (bench_batched, reference_batched), "plain-1080p": (bench_plain, reference_plain),
              "video-4k": (bench_video, reference_video), "served": (bench_served, reference_served),
-             "c0": (bench_c0, reference_c0)}
+             "c0": (bench_c0, reference_c0), "next-rows": (bench_next, None)}
 # The other configs, reported as sub-objects of the batched-mixed line's
 # config when it runs on one GPU (the headline stays batched-mixed).
-SUBS = [("c0", "c0"), ("plain_1080p", "plain-1080p"), ("video_4k", "video-4k"), ("served", "served")]
+SUBS = [("c0", "c0"), ("plain_1080p", "plain-1080p"), ("video_4k", "video-4k"), ("served", "served"),
+        ("next_rows", "next-rows")]
 SUB_DROP = ("metric", "n_gpus", "higher_is_better", "scaling", "vs_baseline", "data")
 
 
 def sub_line(line):
+    if "metric" not in line:
+        return line
     return {k: v for k, v in line.items() if k not in SUB_DROP}
 
 
@@ -1309,15 +1411,22 @@ def main():
     if args.impl == "reference":
         if int(os.environ.get("RANK", "0")) != 0:
             return 0
+        if ref is None:
+            print(json.dumps({"impl": "reference", "unavailable": f"{args.workload}: timed against the oracle inside "
+                              "the GPU arm's line"}), flush=True)
+            return 0
         line = ref(args)
         if subs:
             for key, wl in SUBS:
-                line["config"][key] = sub_line(WORKLOADS[wl][1](args))
+                if WORKLOADS[wl][1] is not None:
+                    line["config"][key] = sub_line(WORKLOADS[wl][1](args))
         print(json.dumps(line), flush=True)
         return 0
     args.warmup = max(3, args.warmup)
     ctx = Ctx(args)
     line = ours(args, ctx)
+    if "metric" not in line:  # a section of the full line run on its own
+        line = {"metric": METRIC, "config": line}
     if subs and ctx.world == 1:
         sub_args = argparse.Namespace(**vars(args))
         sub_args.tuning = None

@@ -79,6 +79,35 @@ int visar_morphology(const visar_image *src, const visar_image *dst, int op, int
 /* include/visar.h:75, src/capi.zig:372-380. interpolation 0 nearest, else linear. */
 int visar_warp_affine(const visar_image *src, const visar_image *dst, const double m[6], int interpolation, int border, double value);
 
+/* include/visar.h:53, src/capi.zig:176-182 -> src/videoio/frame.zig:169-174.
+   BT.601 gray of a BGR or BGRA 8U image shrunk by the integer factor k (1-16)
+   with box averaging, in one pass; dst is (width / k) x (height / k), 1 channel,
+   leftover columns and rows are ignored. k <= 0: InvalidArgument; k > 16 or
+   other shapes: SizeMismatch. */
+int visar_gray_downsample(const visar_image *src, const visar_image *dst, int k);
+
+/* include/visar.h:58-60, src/capi.zig:234-249 -> src/imgproc/pyramid.zig:73, :408.
+   Types 8U, 16U, 16S, 32F, any channel count. pyr_down: dst ((w+1)/2, (h+1)/2),
+   border 1-4 (BORDER_CONSTANT: Unsupported); pyr_up: dst (2w, 2h), border must be
+   4 (BORDER_REFLECT_101). */
+int visar_pyr_down(const visar_image *src, const visar_image *dst, int border);
+int visar_pyr_up(const visar_image *src, const visar_image *dst, int border);
+
+/* include/visar.h:333-341, src/capi_calib3d.zig:186-213 -> src/calib3d/undistort.zig.
+   dist: nd = 0, 4, 5 or 8 coefficients (k1 k2 p1 p2 [k3 [k4 k5 k6]]); a NULL dist
+   is none (InvalidArgument for any other nd).
+   undistort: 8U, 1-4 channels, dst the shape of src; new_k may be NULL (= k).
+   init_undistort_rectify_map: VISAR_32F one-channel maps of equal shape; r and
+   new_k may be NULL (identity / k); a singular new_k * r is InvalidArgument.
+   remap: 8U 1-4 channels through VISAR_32F one-channel maps the size of dst,
+   INTER_LINEAR, BORDER_CONSTANT with `value` (rounded, clamped to 0-255). */
+int visar_undistort(const visar_image *src, const visar_image *dst, const double k[9], const double *dist, size_t nd,
+                    const double *new_k);
+int visar_init_undistort_rectify_map(const double k[9], const double *dist, size_t nd, const double *r, const double *new_k,
+                                     const visar_image *mapx, const visar_image *mapy);
+int visar_remap(const visar_image *src, const visar_image *dst, const visar_image *mapx, const visar_image *mapy,
+                double value);
+
 /* Additive exports (Zig API only in VISAR, no C entry point there). */
 /* src/imgproc/geometry.zig:586-589 warpPerspective(exec, src, dst, [9]f64, WarpInterp, Border, f64) */
 int visar_warp_perspective(const visar_image *src, const visar_image *dst, const double m[9], int interpolation, int border, double value);

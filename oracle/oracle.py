@@ -151,6 +151,76 @@ def resize_generic_u8(a, size, interpolation=1):
     return dst
 
 
+def gray_downsample(a, k, dst=None):
+    """grayDownsample (frame.zig:169-335): BGR/BGRA u8 -> (w // k) x (h // k) gray."""
+    if dst is None:
+        dst = np.empty((a.shape[0] // k if k > 0 else 0, a.shape[1] // k if k > 0 else 0), np.uint8)
+    _check(lib.oracle_gray_downsample(ctypes.byref(desc(a)), ctypes.byref(desc(dst)), int(k)))
+    return dst
+
+
+def pyr_down(a, border=4, dst=None):
+    if dst is None:
+        dst = np.empty(_shape(a, (a.shape[1] + 1) // 2, (a.shape[0] + 1) // 2), a.dtype)
+    _check(lib.oracle_pyr_down(ctypes.byref(desc(a)), ctypes.byref(desc(dst)), int(border)))
+    return dst
+
+
+def pyr_up(a, border=4, dst=None):
+    if dst is None:
+        dst = np.empty(_shape(a, 2 * a.shape[1], 2 * a.shape[0]), a.dtype)
+    _check(lib.oracle_pyr_up(ctypes.byref(desc(a)), ctypes.byref(desc(dst)), int(border)))
+    return dst
+
+
+_DP = ctypes.POINTER(ctypes.c_double)
+lib.oracle_undistort.argtypes = [ctypes.c_void_p, ctypes.c_void_p, _DP, _DP, ctypes.c_size_t, _DP]
+lib.oracle_init_undistort_rectify_map.argtypes = [_DP, _DP, ctypes.c_size_t, _DP, _DP, ctypes.c_void_p, ctypes.c_void_p]
+lib.oracle_remap.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double]
+
+
+def _dv(v, n=None):
+    if v is None:
+        return None, 0
+    a = np.ascontiguousarray(np.asarray(v, np.float64).ravel())
+    if n is not None and a.size != n:
+        raise ValueError(f"expected {n} values")
+    return a, a.size
+
+
+def _pp(a):
+    return None if a is None else a.ctypes.data_as(_DP)
+
+
+def undistort(a, k, dist=None, new_k=None, dst=None):
+    dst = np.empty_like(a) if dst is None else dst
+    km, _ = _dv(k, 9)
+    dv, nd = _dv(dist)
+    nk, _ = _dv(new_k, 9)
+    _check(lib.oracle_undistort(ctypes.byref(desc(a)), ctypes.byref(desc(dst)), _pp(km), _pp(dv), nd, _pp(nk)))
+    return dst
+
+
+def init_undistort_rectify_map(k, dist, r, new_k, size):
+    w, h = size
+    mx = np.empty((h, w), np.float32)
+    my = np.empty((h, w), np.float32)
+    km, _ = _dv(k, 9)
+    dv, nd = _dv(dist)
+    rm, _ = _dv(r, 9)
+    nk, _ = _dv(new_k, 9)
+    _check(lib.oracle_init_undistort_rectify_map(_pp(km), _pp(dv), nd, _pp(rm), _pp(nk), ctypes.byref(desc(mx)),
+                                                 ctypes.byref(desc(my))))
+    return mx, my
+
+
+def remap(a, mapx, mapy, value=0.0, dst=None):
+    dst = np.empty(_shape(a, mapx.shape[1], mapx.shape[0]), np.uint8) if dst is None else dst
+    _check(lib.oracle_remap(ctypes.byref(desc(a)), ctypes.byref(desc(dst)), ctypes.byref(desc(mapx)), ctypes.byref(desc(mapy)),
+                            ctypes.c_double(value)))
+    return dst
+
+
 def morphology(a, op, shape, ksize, iterations=1, dst=None):
     dst = np.empty_like(a) if dst is None else dst
     _check(lib.oracle_morphology(ctypes.byref(desc(a)), ctypes.byref(desc(dst)), op, shape, ksize[0], ksize[1], iterations))

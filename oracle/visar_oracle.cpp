@@ -1691,6 +1691,186 @@ void morphology_t(const visar_image *src, const visar_image *dst, int depth, int
   }
 }
 
+// ================================================================ pyramids
+
+// Exact accumulators of pyramid.zig:25-33 (u8 -> u16, u16 -> u32, i16 -> i32,
+// f32 -> f32); int64 / float here.
+template <class T> struct PAcc { using A = int64_t; };
+template <> struct PAcc<float> { using A = float; };
+
+template <class T, class A>
+T pfinish(A v, int s) {
+  if constexpr (std::is_same<A, float>::value) return v * (1.0f / (float)(1 << s));
+  else return (T)((v + (1 << (s - 1))) >> s);
+}
+
+// pyrDown downChunk (pyramid.zig:99-127): vert5 of the five mapped rows into a
+// row padded with two mapped pixels each side, then h5s at every even pixel.
+template <class T>
+void pyr_down_t(const Img<T> &s, const Img<T> &d, int border) {
+  using A = typename PAcc<T>::A;
+  const int cn = s.cn, w = s.w;
+  const size_t n = (size_t)w * cn, pad = 2 * (size_t)cn;
+  int lmap[2], rmap[2];
+  for (int i = 0; i < 2; i++) {
+    lmap[i] = (int)border_map(i - 2, w, border);
+    rmap[i] = (int)border_map(w + i, w, border);
+  }
+  parallel_for(d.h, 2, [&](size_t y0, size_t y1) {
+    std::vector<A> p(n + 2 * pad);
+    for (size_t y = y0; y < y1; y++) {
+      const T *r[5];
+      for (int k = 0; k < 5; k++) r[k] = s.row(border_map((long long)(2 * y + k) - 2, s.h, border));
+      A *mid = p.data() + pad;
+      for (size_t x = 0; x < n; x++) {
+        const A a = r[0][x], b = r[1][x], c = r[2][x], e = r[3][x], f = r[4][x];
+        mid[x] = (a + f) + (b + e) * (A)4 + c * (A)6;
+      }
+      for (int i = 0; i < 2; i++)
+        for (int ch = 0; ch < cn; ch++) {
+          p[(size_t)i * cn + ch] = mid[(size_t)lmap[i] * cn + ch];
+          p[pad + n + (size_t)i * cn + ch] = mid[(size_t)rmap[i] * cn + ch];
+        }
+      T *out = d.row(y);
+      for (size_t x = 0; x < d.row_len(); x++) {
+        const size_t e = 2 * x - x % cn;  // padded element of the first tap
+        const A v = (p[e] + p[e + 4 * cn]) + (p[e + cn] + p[e + 3 * cn]) * (A)4 + p[e + 2 * cn] * (A)6;
+        out[x] = pfinish<T, A>(v, 8);
+      }
+    }
+  });
+}
+
+// pyrUp upChunk (pyramid.zig:428-518): vert3 into even / odd rows padded by
+// one pixel each side (pixel -1 is pixel 1, pixel w is pixel w-1), then the
+// even / odd horizontal sums.
+template <class T>
+void pyr_up_t(const Img<T> &s, const Img<T> &d) {
+  using A = typename PAcc<T>::A;
+  const int cn = s.cn, w = s.w, h = s.h;
+  const size_t n = (size_t)w * cn;
+  const int left = w > 1 ? 1 : 0;
+  parallel_for(h, 1, [&](size_t y0, size_t y1) {
+    std::vector<A> qe(n + 2 * cn), qo(n + 2 * cn);
+    for (size_t y = y0; y < y1; y++) {
+      const T *a = s.row(y > 0 ? y - 1 : (h > 1 ? 1 : 0));
+      const T *b = s.row(y);
+      const T *c = s.row(y + 1 < (size_t)h ? y + 1 : y);
+      for (size_t x = 0; x < n; x++) {
+        const A va = a[x], vb = b[x], vc = c[x];
+        qe[cn + x] = (va + vc) + vb * (A)6;
+        qo[cn + x] = (vb + vc) * (A)4;
+      }
+      for (std::vector<A> *q : {&qe, &qo})
+        for (int ch = 0; ch < cn; ch++) {
+          (*q)[ch] = (*q)[(size_t)cn + (size_t)left * cn + ch];
+          (*q)[cn + n + ch] = (*q)[n + ch];
+        }
+      for (int k = 0; k < 2; k++) {
+        const std::vector<A> &q = k == 0 ? qe : qo;
+        T *out = d.row(2 * y + k);
+        for (size_t x = 0; x < n; x++) {
+          const size_t o = 2 * x - x % cn;
+          out[o] = pfinish<T, A>((q[x] + q[x + 2 * cn]) + q[x + cn] * (A)6, 6);
+          out[o + cn] = pfinish<T, A>((q[x + cn] + q[x + 2 * cn]) * (A)4, 6);
+        }
+      }
+    }
+  });
+}
+
+template <class T>
+void pyr_d(const visar_image *src, const visar_image *dst, int depth, int border, bool up) {
+  Img<T> s = typed<T>(src, depth);
+  Img<T> d = typed<T>(dst, depth);
+  if (up) {
+    if (border != 4) fail(VISAR_UNSUPPORTED, "Unsupported");
+    if (d.cn != s.cn || d.w != 2 * s.w || d.h != 2 * s.h) fail(VISAR_SIZE_MISMATCH, "SizeMismatch");
+    pyr_up_t(s, d);
+  } else {
+    if (border == 0) fail(VISAR_UNSUPPORTED, "Unsupported");
+    if (d.cn != s.cn || d.w != (s.w + 1) / 2 || d.h != (s.h + 1) / 2) fail(VISAR_SIZE_MISMATCH, "SizeMismatch");
+    pyr_down_t(s, d, border);
+  }
+}
+
+// ======================================================= undistort / remap
+
+// linalg.inv3 / mul3 (src/calib3d/linalg.zig:417-438).
+bool inv3(const double a[9], double out[9]) {
+  const double det = a[0] * (a[4] * a[8] - a[7] * a[5]) - a[1] * (a[3] * a[8] - a[6] * a[5]) + a[2] * (a[3] * a[7] - a[6] * a[4]);
+  if (det == 0) return false;
+  const double d = 1 / det;
+  const double r[9] = {(a[4] * a[8] - a[5] * a[7]) * d, (a[2] * a[7] - a[1] * a[8]) * d, (a[1] * a[5] - a[2] * a[4]) * d,
+                       (a[5] * a[6] - a[3] * a[8]) * d, (a[0] * a[8] - a[2] * a[6]) * d, (a[2] * a[3] - a[0] * a[5]) * d,
+                       (a[3] * a[7] - a[4] * a[6]) * d, (a[1] * a[6] - a[0] * a[7]) * d, (a[0] * a[4] - a[1] * a[3]) * d};
+  std::memcpy(out, r, sizeof(r));
+  return true;
+}
+
+void mul3(const double a[9], const double b[9], double r[9]) {
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) r[i * 3 + j] = a[i * 3] * b[j] + a[i * 3 + 1] * b[3 + j] + a[i * 3 + 2] * b[6 + j];
+}
+
+// MapParams (undistort.zig:26-81).
+struct MapP {
+  double ir[9], fx, fy, u0, v0, k[8];
+  void map(double i, double j, double &u, double &v) const {
+    double x = (i * ir[1] + ir[2]) + j * ir[0];
+    double y = (i * ir[4] + ir[5]) + j * ir[3];
+    if (!(ir[6] == 0 && ir[7] == 0 && ir[8] == 1)) {
+      const double w = 1.0 / ((i * ir[7] + ir[8]) + j * ir[6]);
+      x = x * w;
+      y = y * w;
+    }
+    const double x2 = x * x, y2 = y * y, r2 = x2 + y2, xy2 = 2 * x * y;
+    double kr = 1 + ((k[4] * r2 + k[1]) * r2 + k[0]) * r2;
+    if (k[5] != 0 || k[6] != 0 || k[7] != 0) kr /= 1 + ((k[7] * r2 + k[6]) * r2 + k[5]) * r2;
+    const double xd = x * kr + k[2] * xy2 + k[3] * (r2 + 2 * x2);
+    const double yd = y * kr + k[2] * (r2 + 2 * y2) + k[3] * xy2;
+    u = fx * xd + u0;
+    v = fy * yd + v0;
+  }
+};
+
+MapP map_params(const double ir[9], const double K[9], const double k8[8]) {
+  MapP p;
+  std::memcpy(p.ir, ir, sizeof(p.ir));
+  p.fx = K[0];
+  p.fy = K[4];
+  p.u0 = K[2];
+  p.v0 = K[5];
+  std::memcpy(p.k, k8, sizeof(p.k));
+  return p;
+}
+
+// fix (undistort.zig:114-122): round(v * 32) half to even, clamped.
+int fix32(double v) {
+  const double c = std::min(std::max(v * 32, -2147483647.0), 2147483647.0);
+  return (int)std::nearbyint(c);
+}
+
+// sample (undistort.zig:124-172): 15-bit fixed-point bilinear, border 0.
+void sample_fixed(const Img<uint8_t> &s, int iu, int iv, uint8_t *o) {
+  const int cn = s.cn, W = s.w, H = s.h;
+  const int sx = iu >> 5, sy = iv >> 5, a = iu & 31, b = iv & 31;
+  const int w[4] = {(32 - a) * (32 - b), a * (32 - b), (32 - a) * b, a * b};
+  if (sx >= W || sx + 1 < 0 || sy >= H || sy + 1 < 0) {
+    for (int c = 0; c < cn; c++) o[c] = 0;
+    return;
+  }
+  for (int c = 0; c < cn; c++) {
+    int sum = 0;
+    for (int q = 0; q < 4; q++) {
+      const int px = sx + (q & 1), py = sy + (q >> 1);
+      const int v = (px >= 0 && px < W && py >= 0 && py < H) ? s.row(py)[(size_t)px * cn + c] : 0;
+      sum += v * w[q];
+    }
+    o[c] = (uint8_t)((sum + 512) >> 10);
+  }
+}
+
 // ============================================================== dispatch
 
 int src_depth(const visar_image *c) {
@@ -1814,6 +1994,45 @@ int oracle_resize(const visar_image *src, const visar_image *dst, int interp) {
   });
 }
 
+// grayDownsample (src/videoio/frame.zig:169-335): per output pixel the k x k
+// block sums of B, G and R (alpha ignored), l = sb*1868 + sg*9617 + sr*4899
+// (u32); k == 2 rounds (l + 2^15) >> 16 (`pairs`), every other k truncates
+// min(255, f32(l) * f32(1 / (k*k*2^14)) + 0.5) (`blocks`, f32 steps unfused).
+int oracle_gray_downsample(const visar_image *src, const visar_image *dst, int k) {
+  return guarded([&] {
+    if (k <= 0) fail(VISAR_INVALID_ARGUMENT, "InvalidArgument");
+    Img<uint8_t> s = typed<uint8_t>(src, 0);
+    Img<uint8_t> d = typed<uint8_t>(dst, 0);
+    if (k > 16 || d.cn != 1 || (s.cn != 3 && s.cn != 4)) fail(VISAR_SIZE_MISMATCH, "SizeMismatch");
+    if (d.w != s.w / k || d.h != s.h / k) fail(VISAR_SIZE_MISMATCH, "SizeMismatch");
+    const int cn = s.cn;
+    const float inv = 1.0f / (float)(k * k * (1 << 14));
+    parallel_for(d.h, 8, [&](size_t y0, size_t y1) {
+      for (size_t oy = y0; oy < y1; oy++) {
+        uint8_t *o = d.row(oy);
+        for (int ox = 0; ox < d.w; ox++) {
+          uint32_t sb = 0, sg = 0, sr = 0;
+          for (int dy = 0; dy < k; dy++) {
+            const uint8_t *r = s.row(oy * k + dy) + (size_t)ox * k * cn;
+            for (int dx = 0; dx < k; dx++) {
+              sb += r[dx * cn];
+              sg += r[dx * cn + 1];
+              sr += r[dx * cn + 2];
+            }
+          }
+          const uint32_t l = sb * 1868u + sg * 9617u + sr * 4899u;
+          if (k == 2) {
+            o[ox] = (uint8_t)((l + (1u << 15)) >> 16);
+          } else {
+            const float f = std::min(255.0f, (float)l * inv + 0.5f);
+            o[ox] = (uint8_t)(uint32_t)f;
+          }
+        }
+      }
+    });
+  });
+}
+
 // The generic kernels VISAR's resize tests compare its dispatch against
 // (resize.zig:654-682 `linear`, :701-743 `areaGeneric`); u8 only.
 int oracle_resize_generic_u8(const visar_image *src, const visar_image *dst, int interp) {
@@ -1824,6 +2043,134 @@ int oracle_resize_generic_u8(const visar_image *src, const visar_image *dst, int
     if (interp == 1) linear_generic_u8(s, d, false);
     else if (interp == 3) area_generic(s, d);
     else fail(VISAR_UNSUPPORTED, "Unsupported");
+  });
+}
+
+int oracle_pyr_down(const visar_image *src, const visar_image *dst, int border) {
+  return guarded([&] {
+    check_border(border);
+    const int depth = src_depth(src);
+    ORACLE_DISPATCH(depth, pyr_d, src, dst, depth, border, false);
+  });
+}
+
+int oracle_pyr_up(const visar_image *src, const visar_image *dst, int border) {
+  return guarded([&] {
+    check_border(border);
+    const int depth = src_depth(src);
+    ORACLE_DISPATCH(depth, pyr_d, src, dst, depth, border, true);
+  });
+}
+
+void expand_dist(const double *dist, size_t nd, double k8[8]) {
+  for (int i = 0; i < 8; i++) k8[i] = 0;
+  if (!dist) return;
+  if (nd != 0 && nd != 4 && nd != 5 && nd != 8) fail(VISAR_INVALID_ARGUMENT, "InvalidArgument");
+  for (size_t i = 0; i < nd; i++) k8[i] = dist[i];
+}
+
+// undistort (undistort.zig:204-281): stripes of min(max(1, 4096 / w), h) rows,
+// the new camera's v0 moved up by the stripe's first row.
+int oracle_undistort(const visar_image *src, const visar_image *dst, const double K[9], const double *dist, size_t nd,
+                     const double *new_k) {
+  return guarded([&] {
+    Img<uint8_t> s = typed<uint8_t>(src, 0);
+    Img<uint8_t> d = typed<uint8_t>(dst, 0);
+    if (!K) fail(VISAR_INVALID_ARGUMENT, "InvalidArgument");
+    if (s.w != d.w || s.h != d.h || s.cn != d.cn) fail(VISAR_SIZE_MISMATCH, "SizeMismatch");
+    if (s.cn < 1 || s.cn > 4) fail(VISAR_UNSUPPORTED, "Unsupported");
+    double k8[8];
+    expand_dist(dist, nd, k8);
+    const double *ar0 = new_k ? new_k : K;
+    const int stripe = std::min(std::max(1, 4096 / std::max(s.w, 1)), s.h);
+    const int nstripes = (s.h + stripe - 1) / stripe;
+    parallel_for(nstripes, 1, [&](size_t s0, size_t s1) {
+      for (size_t st = s0; st < s1; st++) {
+        const int y0 = (int)st * stripe, y1 = std::min(y0 + stripe, s.h);
+        double ar[9], ir[9];
+        std::memcpy(ar, ar0, sizeof(ar));
+        ar[5] = ar0[5] - (double)y0;
+        if (!inv3(ar, ir)) continue;  // the stripe is left as it is
+        const MapP p = map_params(ir, K, k8);
+        for (int y = y0; y < y1; y++) {
+          uint8_t *o = d.row(y);
+          for (int x = 0; x < d.w; x++) {
+            double u, v;
+            p.map((double)(y - y0), (double)x, u, v);
+            sample_fixed(s, fix32(u), fix32(v), o + (size_t)x * s.cn);
+          }
+        }
+      }
+    });
+  });
+}
+
+int oracle_init_undistort_rectify_map(const double K[9], const double *dist, size_t nd, const double *R, const double *new_k,
+                                      const visar_image *mapx, const visar_image *mapy) {
+  return guarded([&] {
+    Img<float> mx = typed<float>(mapx, 5);
+    Img<float> my = typed<float>(mapy, 5);
+    if (!K) fail(VISAR_INVALID_ARGUMENT, "InvalidArgument");
+    double k8[8];
+    expand_dist(dist, nd, k8);
+    const double eye[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    double m[9], ir[9];
+    mul3(new_k ? new_k : K, R ? R : eye, m);
+    if (!inv3(m, ir)) fail(VISAR_INVALID_ARGUMENT, "InvalidArgument");
+    if (mx.w != my.w || mx.h != my.h || mx.cn != my.cn || mx.cn != 1) fail(VISAR_SIZE_MISMATCH, "SizeMismatch");
+    const MapP p = map_params(ir, K, k8);
+    parallel_for(mx.h, 16, [&](size_t y0, size_t y1) {
+      for (size_t y = y0; y < y1; y++)
+        for (int x = 0; x < mx.w; x++) {
+          double u, v;
+          p.map((double)y, (double)x, u, v);
+          mx.row(y)[x] = (float)u;
+          my.row(y)[x] = (float)v;
+        }
+    });
+  });
+}
+
+// remap -> linearF32 (undistort.zig:288-392).
+int oracle_remap(const visar_image *src, const visar_image *dst, const visar_image *mapx, const visar_image *mapy, double value) {
+  return guarded([&] {
+    Img<uint8_t> s = typed<uint8_t>(src, 0);
+    Img<uint8_t> d = typed<uint8_t>(dst, 0);
+    Img<float> mx = typed<float>(mapx, 5);
+    Img<float> my = typed<float>(mapy, 5);
+    const double rv = std::round(value);
+    const uint8_t bv = (uint8_t)(rv != rv ? 0 : std::min(255.0, std::max(0.0, rv)));
+    if (d.w != mx.w || d.h != mx.h || mx.w != my.w || mx.h != my.h || mx.cn != my.cn || mx.cn != 1)
+      fail(VISAR_SIZE_MISMATCH, "SizeMismatch");
+    if (s.cn != d.cn || s.cn < 1 || s.cn > 4) fail(VISAR_UNSUPPORTED, "Unsupported");
+    const int cn = s.cn;
+    parallel_for(d.h, 8, [&](size_t y0, size_t y1) {
+      for (size_t y = y0; y < y1; y++) {
+        uint8_t *o = d.row(y);
+        for (int x = 0; x < d.w; x++) {
+          const float sx = mx.row(y)[x], sy = my.row(y)[x];
+          const float fx = std::floor(sx), fy = std::floor(sy);
+          uint8_t *op = o + (size_t)x * cn;
+          if (!(fx >= -1 && fy >= -1 && fx < (float)s.w && fy < (float)s.h)) {
+            for (int c = 0; c < cn; c++) op[c] = bv;
+            continue;
+          }
+          const float ax = sx - fx, ay = sy - fy;
+          const int ix = (int)fx, iy = (int)fy;
+          for (int c = 0; c < cn; c++) {
+            float p[4];
+            for (int q = 0; q < 4; q++) {
+              const int px = ix + (q & 1), py = iy + (q >> 1);
+              p[q] = (px >= 0 && px < s.w && py >= 0 && py < s.h) ? (float)s.row(py)[(size_t)px * cn + c] : (float)bv;
+            }
+            const float v0 = std::fma(ax, p[1] - p[0], p[0]);
+            const float v1 = std::fma(ax, p[3] - p[2], p[2]);
+            const float v = std::fma(ay, v1 - v0, v0);
+            op[c] = (uint8_t)std::min(std::max(std::nearbyint(v), 0.0f), 255.0f);
+          }
+        }
+      }
+    });
   });
 }
 

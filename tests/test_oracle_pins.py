@@ -335,3 +335,169 @@ def test_sep_filter_2d_even_kernels_refused():
         with pytest.raises(O.OracleError) as e:
             O.sep_filter_2d(a, np.uint8, kx, ky, 4)
         assert e.value.status == -1 and "InvalidKernel" in e.value.name
+
+
+# ------------------------------------------------------------ gray + integer shrink
+
+def _luma_mean(src, k):
+    h, w = src.shape[0] // k * k, src.shape[1] // k * k
+    s = src[:h, :w].astype(np.float64)
+    lum = (s[..., 0] * 1868 + s[..., 1] * 9617 + s[..., 2] * 4899) / 16384.0
+    return lum.reshape(h // k, k, w // k, k).mean(axis=(1, 3))
+
+
+@pytest.mark.parametrize("cn", [4, 3])
+def test_gray_downsample_matches_gray_then_area(cn):
+    # frame.zig:384-416: within 0.51 of the f64 mean of per-pixel lumas; at
+    # k = 1 within 1 of cvtColor's gray.
+    for k in (1, 2, 3, 4, 6, 8):
+        rng = np.random.default_rng(k)
+        src = rng.integers(0, 256, (9 * k, 70 * k + 1, cn), dtype=np.uint8)
+        d = O.gray_downsample(src, k)
+        assert d.shape == (9, 70 + (k == 1))
+        assert np.abs(d - _luma_mean(src, k)).max() <= 0.51, (cn, k)
+        if k == 1:
+            g = O.cvt_color(src, 10 if cn == 4 else 6)
+            assert np.abs(d.astype(int) - g.astype(int)).max() <= 1
+
+
+def test_gray_downsample_refusals():
+    src = np.zeros((40, 50, 3), np.uint8)
+    for k, shape, want in [(0, (40, 50), (-1, "InvalidArgument")), (17, (2, 2), (-2, "SizeMismatch")),
+                           (2, (20, 24), (-2, "SizeMismatch")), (2, (20, 25, 3), (-2, "SizeMismatch"))]:
+        with pytest.raises(O.OracleError) as e:
+            O.gray_downsample(src, k, dst=np.zeros(shape, np.uint8))
+        assert (e.value.status, e.value.name) == want, (k, shape)
+    with pytest.raises(O.OracleError) as e:
+        O.gray_downsample(np.zeros((40, 50), np.uint8), 2)
+    assert e.value.status == -2
+
+
+# ------------------------------------------------------------------------ pyramids
+
+import pins_pyr as PP  # noqa: E402
+
+PYR_TYPES = [np.uint8, np.uint16, np.int16, np.float32]
+PYR_SIZES = [(1, 1), (2, 3), (5, 4), (37, 19), (70, 9), (129, 7)]  # (w, h), pyramid.zig:626
+
+
+@pytest.mark.parametrize("dtype", PYR_TYPES)
+def test_pyr_down_up_equal_direct_sums(dtype):
+    # pyramid.zig:624-644 (channel counts 1-5, every border but constant).
+    for w, h in PYR_SIZES:
+        for cn in (1, 2, 3, 4, 5):
+            src = PP.fill_random(dtype, w, h, cn, w * 31 + cn)
+            for b in (4, 2, 1, 3):
+                got = O.pyr_down(src, b).reshape((h + 1) // 2, (w + 1) // 2, cn)
+                want = PP.ref_down(src, b)
+                if dtype == np.float32:
+                    assert np.abs(got - want).max() <= 1e-5, (w, h, cn, b)
+                else:
+                    assert np.array_equal(got.astype(np.int64), want.astype(np.int64)), (w, h, cn, b)
+            got = O.pyr_up(src, 4).reshape(2 * h, 2 * w, cn)
+            want = PP.ref_up(src)
+            if dtype == np.float32:
+                assert np.abs(got - want).max() <= 1e-5, (w, h, cn)
+            else:
+                assert np.array_equal(got.astype(np.int64), want.astype(np.int64)), (w, h, cn)
+
+
+def test_pyr_down_f32_scalar_order():
+    # pyramid.zig:646-672: f32 3/4 channels equal the scalar formula exactly.
+    for w, h in [(131, 12), (64, 9), (70, 7), (9, 5)]:
+        for cn in (3, 4):
+            src = PP.fill_random(np.float32, w, h, cn, w * 7 + cn)
+            for b in (4, 1):
+                got = O.pyr_down(src, b).reshape((h + 1) // 2, (w + 1) // 2, cn)
+                assert np.array_equal(got, PP.down_f32_scalar(src, b)), (w, h, cn, b)
+
+
+def test_pyramid_sizes_and_refusals():
+    # pyramid.zig:674-688: levels of 101x50 are 51x25 ... 7x4; a constant image stays constant.
+    lv = np.full((50, 101), 7, np.uint8)
+    sizes = []
+    for _ in range(4):
+        lv = O.pyr_down(lv, 4)
+        sizes.append(lv.shape)
+    assert sizes == [(25, 51), (13, 26), (7, 13), (4, 7)] and (lv == 7).all()
+    src = np.zeros((50, 101), np.uint8)
+    for fn, dst, border, want in [(O.pyr_down, np.zeros((13, 26), np.uint8), 4, -2),
+                                  (O.pyr_down, np.zeros((25, 51), np.uint8), 0, -3),
+                                  (O.pyr_up, np.zeros((100, 202), np.uint8), 1, -3),
+                                  (O.pyr_up, np.zeros((100, 201), np.uint8), 4, -2),
+                                  (O.pyr_down, np.zeros((25, 51), np.uint8), 5, -3)]:
+        with pytest.raises(O.OracleError) as e:
+            fn(src, border, dst=dst)
+        assert e.value.status == want, (fn.__name__, dst.shape, border)
+
+
+# --------------------------------------------------------------- undistort / remap
+
+import pins_calib as PC  # noqa: E402
+
+
+def test_undistort_zero_distortion_is_identity():
+    # undistort.zig:396-408: all but the last row and column come back unchanged.
+    src = (np.arange(23 * 37 * 3) * 7 % 256).astype(np.uint8).reshape(23, 37, 3)
+    d = O.undistort(src, [40, 0, 18, 0, 40, 11, 0, 0, 1], [])
+    assert np.array_equal(d[:22, :36], src[:22, :36])
+
+
+@pytest.mark.parametrize("cn", [1, 2, 3, 4])
+def test_undistort_and_maps_equal_cv2(cn):
+    import cv2
+    rng = np.random.default_rng(cn)
+    for w, h in [(640, 480), (97, 61), (1500, 1000), (4100, 9)]:
+        img = rng.integers(0, 256, (h, w, cn), dtype=np.uint8)
+        img = img[..., 0] if cn == 1 else img
+        for K0, dist, nk in PC.CAMERAS:
+            K = PC.scaled_camera(K0, w, h)
+            d = np.array(dist) if dist else None
+            ours = O.undistort(img, K, dist, nk)
+            ref = cv2.undistort(img, K, d, newCameraMatrix=nk)
+            # Equal but where a source coordinate lies within 1e-6 of a 1/64
+            # pixel boundary (OpenCV's own map arithmetic may round it the
+            # other way; undistort.zig:7-11).
+            for y, x in {(int(a), int(b)) for a, b in np.argwhere((ours != ref).reshape(h, w, -1).any(axis=2))}:
+                u, v = PC.undistort_coord(K, dist, nk, w, h, x, y)
+                assert PC.near_tie(u) or PC.near_tie(v), (cn, w, h, dist, x, y, u, v)
+            if cn == 1:
+                R = np.array([[0.999, -0.01, 0.02], [0.011, 0.9995, -0.005], [-0.02, 0.006, 0.9992]])
+                for r in (None, R):
+                    mx, my = O.init_undistort_rectify_map(K, dist, r, nk, (w, h))
+                    cx, cy = cv2.initUndistortRectifyMap(K, d, r, nk if nk is not None else K, (w, h), cv2.CV_32FC1)
+                    if dist:
+                        # Equal but at f64 values within 1e-9 of an f32 rounding tie.
+                        for axis, (a, b) in enumerate(((mx, cx), (my, cy))):
+                            for y, x in np.argwhere(a != b):
+                                c = PC.undistort_coord(K, dist, nk, w, h, int(x), int(y), R=r, stripes=False)[axis]
+                                assert PC.f32_tie(c, a[y, x], b[y, x]), (w, h, dist, r is None, x, y, c, a[y, x], b[y, x])
+                    else:  # OpenCV inverts an identity-distortion camera by a route that can leave 1e-16 residues
+                        for a, b in ((mx, cx), (my, cy)):
+                            assert np.abs(a - b).max() <= 1e-6 * max(1.0, float(np.abs(b).max())), (w, h, r is None)
+
+
+def test_remap_known_answers():
+    bad = [name for name, src, mx, my, v, exp in PC.remap_cases() if not np.array_equal(O.remap(src, mx, my, v), exp)]
+    assert not bad, bad[:10]
+
+
+def test_undistort_remap_refusals():
+    img = np.zeros((20, 30, 3), np.uint8)
+    K = [40, 0, 15, 0, 40, 10, 0, 0, 1]
+    with pytest.raises(O.OracleError) as e:
+        O.undistort(img, K, [0.1, 0.2])
+    assert e.value.status == -1
+    with pytest.raises(O.OracleError) as e:
+        O.undistort(img, K, [], dst=np.zeros((20, 31, 3), np.uint8))
+    assert e.value.status == -2
+    with pytest.raises(O.OracleError) as e:
+        O.init_undistort_rectify_map([0] * 9, [], None, None, (30, 20))
+    assert e.value.status == -1
+    mx = np.zeros((20, 30), np.float32)
+    with pytest.raises(O.OracleError) as e:
+        O.remap(img, mx, np.zeros((20, 29), np.float32))
+    assert e.value.status == -2
+    with pytest.raises(O.OracleError) as e:
+        O.remap(img, mx, mx, dst=np.zeros((20, 30), np.uint8))
+    assert e.value.status == -3

@@ -52,6 +52,10 @@ def _load():
     lib.visar_last_error.restype = ctypes.c_char_p
     lib.visar_cuda_launch_count.restype = ctypes.c_uint64
     lib.visar_cuda_set_stream.argtypes = [ctypes.c_void_p]
+    dp = ctypes.POINTER(ctypes.c_double)
+    lib.visar_undistort.argtypes = [ctypes.c_void_p, ctypes.c_void_p, dp, dp, ctypes.c_size_t, dp]
+    lib.visar_init_undistort_rectify_map.argtypes = [dp, dp, ctypes.c_size_t, dp, dp, ctypes.c_void_p, ctypes.c_void_p]
+    lib.visar_remap.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double]
     return lib
 
 
@@ -176,6 +180,85 @@ def resize_linear_u8_noalloc(a, dst):
     the caller owns) through visar_resize_linear_u8_noalloc: no device memory
     is allocated by the call; destination sides up to 16384."""
     _check(lib.visar_resize_linear_u8_noalloc(ctypes.byref(desc(a)), ctypes.byref(desc(dst))))
+    return dst
+
+
+def gray_downsample(a, k, dst=None):
+    """visar_gray_downsample: BT.601 gray of a BGR / BGRA u8 image shrunk by the
+    integer factor k (1-16) with box averaging, in one pass."""
+    if dst is None:
+        dst = _out(a, (a.shape[0] // k if k > 0 else 0, a.shape[1] // k if k > 0 else 0))
+    _check(lib.visar_gray_downsample(ctypes.byref(desc(a)), ctypes.byref(desc(dst)), int(k)))
+    return dst
+
+
+def pyr_down(a, border=4, dst=None):
+    """visar_pyr_down: 5x5 Gaussian, then every other row and column; dst is ((w+1)//2, (h+1)//2)."""
+    if dst is None:
+        dst = _out(a, _shape(a, (a.shape[1] + 1) // 2, (a.shape[0] + 1) // 2))
+    _check(lib.visar_pyr_down(ctypes.byref(desc(a)), ctypes.byref(desc(dst)), int(border)))
+    return dst
+
+
+def pyr_up(a, border=4, dst=None):
+    """visar_pyr_up: upsample by 2 and blur with the 5x5 Gaussian times 4; dst is (2w, 2h)."""
+    if dst is None:
+        dst = _out(a, _shape(a, 2 * a.shape[1], 2 * a.shape[0]))
+    _check(lib.visar_pyr_up(ctypes.byref(desc(a)), ctypes.byref(desc(dst)), int(border)))
+    return dst
+
+
+def _dptr(v, n=None):
+    """(pointer, length) of a float64 vector, or (None, 0)."""
+    if v is None:
+        return None, 0
+    a = np.ascontiguousarray(np.asarray(v, np.float64).ravel())
+    if n is not None and a.size != n:
+        raise ValueError(f"expected {n} values")
+    return a, a.size
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def undistort(a, k, dist=None, new_k=None, dst=None):
+    """visar_undistort: 8U images of 1-4 channels; k and new_k 3x3, dist 0/4/5/8 coefficients."""
+    dst = _out(a, tuple(a.shape)) if dst is None else dst
+    km, _ = _dptr(k, 9)
+    dv, nd = _dptr(dist)
+    nk, _ = _dptr(new_k, 9)
+    _check(lib.visar_undistort(ctypes.byref(desc(a)), ctypes.byref(desc(dst)), _p(km), _p(dv), ctypes.c_size_t(nd), _p(nk)))
+    return dst
+
+
+def init_undistort_rectify_map(k, dist, r, new_k, size, mapx=None, mapy=None, like=None):
+    """visar_init_undistort_rectify_map: f32 maps of size (w, h); `like` picks host (NumPy, default) or a CUDA tensor."""
+    w, h = size
+
+    def alloc():
+        if like is not None and _is_torch(like):
+            import torch
+            return torch.empty((h, w), dtype=torch.float32, device=like.device)
+        return np.empty((h, w), np.float32)
+
+    mapx = alloc() if mapx is None else mapx
+    mapy = alloc() if mapy is None else mapy
+    km, _ = _dptr(k, 9)
+    dv, nd = _dptr(dist)
+    rm, _ = _dptr(r, 9)
+    nk, _ = _dptr(new_k, 9)
+    _check(lib.visar_init_undistort_rectify_map(_p(km), _p(dv), ctypes.c_size_t(nd), _p(rm), _p(nk),
+                                                ctypes.byref(desc(mapx)), ctypes.byref(desc(mapy))))
+    return mapx, mapy
+
+
+def remap(a, mapx, mapy, value=0.0, dst=None):
+    """visar_remap: 8U 1-4 channels through f32 maps (INTER_LINEAR, constant border `value`)."""
+    if dst is None:
+        dst = _out(a, _shape(a, mapx.shape[1], mapx.shape[0]))
+    _check(lib.visar_remap(ctypes.byref(desc(a)), ctypes.byref(desc(dst)), ctypes.byref(desc(mapx)),
+                           ctypes.byref(desc(mapy)), ctypes.c_double(value)))
     return dst
 
 

@@ -1005,6 +1005,166 @@ int visar_warp_perspective(const visar_image *src, const visar_image *dst, const
   });
 }
 
+// capi.zig:176-182 -> frame.zig:169-174: k <= 0 is InvalidArgument; a factor
+// above 16, a destination that is not one channel of (w / k) x (h / k), or a
+// source that is not BGR / BGRA is SizeMismatch.
+int visar_gray_downsample(const visar_image *src, const visar_image *dst, int k) {
+  return guarded([&] {
+    if (k <= 0) invalid_arg();
+    std::lock_guard<std::mutex> lk(g_mu);
+    View s = typed(src, k8U);
+    View d = typed(dst, k8U);
+    if (k > 16 || d.c->channels != 1 || (s.c->channels != 3 && s.c->channels != 4)) size_mismatch();
+    if (d.c->width != s.c->width / (uint32_t)k || d.c->height != s.c->height / (uint32_t)k) size_mismatch();
+    Call call = begin_call();
+    stage_in(call, s, kSrc);
+    stage_out(call, d, kDst);
+    if (overlaps(s, d)) detach_src(call, s, kTmp1);
+    ck(launch_gray_downsample(s.dev, d.dev, k, call.st));
+    finish_out(call, d);
+    end_call(call, s.host || d.host);
+  });
+}
+
+// capi.zig:234-249 -> pyramid.zig:73-80, 408-413: the border must be 0-4
+// (Unsupported otherwise), pyrDown refuses BORDER_CONSTANT and pyrUp anything
+// but BORDER_REFLECT_101 (Unsupported); dst must have the source's channels
+// and ((w+1)/2, (h+1)/2) resp. (2w, 2h) pixels (SizeMismatch).
+int visar_pyr_down(const visar_image *src, const visar_image *dst, int border) {
+  return guarded([&] {
+    const int bd = border_arg(border);
+    const int depth = src_depth(src);
+    std::lock_guard<std::mutex> lk(g_mu);
+    View s = typed(src, depth);
+    View d = typed(dst, depth);
+    if (bd == 0) unsupported();
+    if (d.c->channels != s.c->channels || d.c->width != (s.c->width + 1) / 2 || d.c->height != (s.c->height + 1) / 2)
+      size_mismatch();
+    Call call = begin_call();
+    stage_in(call, s, kSrc);
+    stage_out(call, d, kDst);
+    if (overlaps(s, d)) detach_src(call, s, kTmp1);
+    ck(launch_pyr_down(s.dev, d.dev, depth, bd, call.st));
+    finish_out(call, d);
+    end_call(call, s.host || d.host);
+  });
+}
+
+int visar_pyr_up(const visar_image *src, const visar_image *dst, int border) {
+  return guarded([&] {
+    const int bd = border_arg(border);
+    const int depth = src_depth(src);
+    std::lock_guard<std::mutex> lk(g_mu);
+    View s = typed(src, depth);
+    View d = typed(dst, depth);
+    if (bd != 4) unsupported();
+    if (d.c->channels != s.c->channels || (uint64_t)d.c->width != 2ull * s.c->width ||
+        (uint64_t)d.c->height != 2ull * s.c->height)
+      size_mismatch();
+    Call call = begin_call();
+    stage_in(call, s, kSrc);
+    stage_out(call, d, kDst);
+    if (overlaps(s, d)) detach_src(call, s, kTmp1);
+    ck(launch_pyr_up(s.dev, d.dev, depth, call.st));
+    finish_out(call, d);
+    end_call(call, s.host || d.host);
+  });
+}
+
+// camera.expandDist (src/calib3d/camera.zig:17-22) of distSlice
+// (capi_calib3d.zig:93-95): a null `dist` is no coefficients; 0, 4, 5 or 8.
+void expand_dist(const double *dist, size_t nd, double k8[8]) {
+  for (int i = 0; i < 8; i++) k8[i] = 0;
+  if (!dist) return;
+  if (nd != 0 && nd != 4 && nd != 5 && nd != 8) invalid_arg();
+  for (size_t i = 0; i < nd; i++) k8[i] = dist[i];
+}
+
+// capi_calib3d.zig:186-191 -> undistort.zig:204-209.
+int visar_undistort(const visar_image *src, const visar_image *dst, const double k[9], const double *dist, size_t nd,
+                    const double *new_k) {
+  return guarded([&] {
+    std::lock_guard<std::mutex> lk(g_mu);
+    View s = typed(src, k8U);
+    View d = typed(dst, k8U);
+    if (!k) invalid_arg();
+    if (s.c->width != d.c->width || s.c->height != d.c->height || s.c->channels != d.c->channels) size_mismatch();
+    if (s.c->channels < 1 || s.c->channels > 4) unsupported();
+    double k8[8];
+    expand_dist(dist, nd, k8);
+    std::vector<uint8_t> stripes;
+    const bool keeps_rows = undistort_stripes(k, k8, new_k, (int)s.c->width, (int)s.c->height, stripes);
+    Call call = begin_call();
+    const void *tab = upload(call, kTab1, stripes);
+    stage_in(call, s, kSrc);
+    if (d.host && keeps_rows) {
+      // Rows under a singular stripe camera are left as they are: start from dst.
+      View dd = d;
+      stage_in(call, dd, kDst);
+      d.dev = dd.dev;
+    } else {
+      stage_out(call, d, kDst);
+    }
+    if (overlaps(s, d)) detach_src(call, s, kTmp1);
+    ck(launch_undistort(s.dev, d.dev, tab, call.st));
+    finish_out(call, d);
+    end_call(call, s.host || d.host);
+  });
+}
+
+// capi_calib3d.zig:195-201: maps VISAR_32F, one channel, of equal shape.
+int visar_init_undistort_rectify_map(const double k[9], const double *dist, size_t nd, const double *r, const double *new_k,
+                                     const visar_image *mapx, const visar_image *mapy) {
+  return guarded([&] {
+    std::lock_guard<std::mutex> lk(g_mu);
+    View mx = typed(mapx, k32F);
+    View my = typed(mapy, k32F);
+    if (!k) invalid_arg();
+    double k8[8];
+    expand_dist(dist, nd, k8);
+    std::vector<uint8_t> params;
+    if (!undistort_map_params(k, k8, r, new_k, params)) invalid_arg();
+    if (mx.c->width != my.c->width || mx.c->height != my.c->height || mx.c->channels != my.c->channels ||
+        mx.c->channels != 1)
+      size_mismatch();
+    Call call = begin_call();
+    stage_out(call, mx, kDst);
+    stage_out(call, my, kTmp2);
+    ck(launch_init_undistort_map(params, mx.dev, my.dev, call.st));
+    finish_out(call, mx);
+    finish_out(call, my);
+    end_call(call, mx.host || my.host);
+  });
+}
+
+// capi_calib3d.zig:205-213 -> undistort.zig:288-291: value rounded half away
+// from zero and clamped to 0..255 for every channel.
+int visar_remap(const visar_image *src, const visar_image *dst, const visar_image *mapx, const visar_image *mapy,
+                double value) {
+  return guarded([&] {
+    std::lock_guard<std::mutex> lk(g_mu);
+    View s = typed(src, k8U);
+    View d = typed(dst, k8U);
+    View mx = typed(mapx, k32F);
+    View my = typed(mapy, k32F);
+    const double rv = std::round(value);
+    const uint8_t bv = (uint8_t)(rv != rv ? 0 : rv < 0 ? 0 : rv > 255 ? 255 : rv);
+    if (d.c->width != mx.c->width || d.c->height != mx.c->height || mx.c->width != my.c->width ||
+        mx.c->height != my.c->height || mx.c->channels != my.c->channels || mx.c->channels != 1)
+      size_mismatch();
+    if (s.c->channels != d.c->channels || s.c->channels < 1 || s.c->channels > 4) unsupported();
+    Call call = begin_call();
+    stage_in(call, s, kSrc);
+    stage_in(call, mx, kTmp2);
+    stage_in(call, my, kTmp3);
+    stage_out(call, d, kDst);
+    if (overlaps(s, d)) detach_src(call, s, kTmp1);
+    ck(launch_remap(s.dev, d.dev, mx.dev, my.dev, bv, call.st));
+    finish_out(call, d);
+    end_call(call, s.host || d.host || mx.host || my.host);
+  });
+}
+
 // visar_resize(src, dst, INTER_LINEAR) for u8 device images without any
 // device allocation: the tap tables go to a static device buffer
 // (noalloc.cu). Host images would need staging buffers and overlapping images

@@ -1,0 +1,254 @@
+// Gaussian pyramid steps (src/imgproc/pyramid.zig): pyrDown (:73-96) and
+// pyrUp (:408-426) for u8 / u16 / i16 / f32 images of any channel count.
+//
+// pyrDown: out(x, y) = sum over i, j in 0..4 of k_i k_j src(map(2x+i-2),
+// map(2y+j-2)), k = [1 4 6 4 1], coordinates mapped by the border rule;
+// integers finish with (v + 128) >> 8 (exact accumulators, so the pass order
+// does not matter), f32 sums vertically first, per column
+// ((r0 + r4) + (r1 + r3) * 4) + r2 * 6, then the same form horizontally, then
+// * (1/256) (pyramid.zig:298-320, 335-344): the same operations in the same
+// order here, each rounded on its own.
+//
+// pyrUp: the same kernel over the source upsampled with zeros and reflected
+// about its own edges: per source row y, even output row 2y takes
+// (r[y-1] + r[y+1]) + r[y] * 6 and odd row 2y+1 takes (r[y] + r[y+1]) * 4
+// (rows mapped: -1 -> 1, h -> h-1); horizontally even pixel 2p takes
+// (q[p-1] + q[p+1]) + q[p] * 6 and odd 2p+1 takes (q[p] + q[p+1]) * 4;
+// integers finish with (v + 32) >> 6, f32 with * (1/64) (pyramid.zig:466-518).
+//
+// Layout: a CTA owns a tile of output rows and pixels. Phase 1 computes the
+// vertical sums of every source element column under the tile (all channels
+// interleaved) into shared memory, coalesced along the row; phase 2 combines
+// them horizontally (taps cn elements apart) and stores the tile. Images with
+// more than 16 channels use a direct kernel (one output element per thread).
+#include "vb.h"
+
+namespace vb {
+namespace {
+
+template <class T> struct PyrAcc { using A = int; };
+template <> struct PyrAcc<float> { using A = float; };
+
+template <class T, int S>
+__device__ __forceinline__ T pyr_finish(int v) {
+  return (T)((v + (1 << (S - 1))) >> S);  // arithmetic shift: floor for negative sums
+}
+template <class T, int S>
+__device__ __forceinline__ T pyr_finish(float v) {
+  return __fmul_rn(v, 1.0f / (float)(1 << S));
+}
+
+// ((a + e) + (b + d) * 4) + c * 6, each step rounded (f32) or exact (int).
+__device__ __forceinline__ int tap5(int a, int b, int c, int d, int e) { return ((a + e) + (b + d) * 4) + c * 6; }
+__device__ __forceinline__ float tap5(float a, float b, float c, float d, float e) {
+  return __fadd_rn(__fadd_rn(__fadd_rn(a, e), __fmul_rn(__fadd_rn(b, d), 4.0f)), __fmul_rn(c, 6.0f));
+}
+__device__ __forceinline__ int up_even(int a, int b, int c) { return (a + c) + b * 6; }
+__device__ __forceinline__ float up_even(float a, float b, float c) { return __fadd_rn(__fadd_rn(a, c), __fmul_rn(b, 6.0f)); }
+__device__ __forceinline__ int up_odd(int b, int c) { return (b + c) * 4; }
+__device__ __forceinline__ float up_odd(float b, float c) { return __fmul_rn(__fadd_rn(b, c), 4.0f); }
+
+template <class T>
+__device__ __forceinline__ typename PyrAcc<T>::A ld(const uint8_t *base, long long stride, int y, int e) {
+  return (typename PyrAcc<T>::A)reinterpret_cast<const T *>(base + (long long)y * stride)[e];
+}
+
+constexpr int kDownRows = 8;      // output rows per tile
+constexpr int kDownElems = 256;   // output elements (pixels x channels) per tile, about
+constexpr int kThreads = 256;
+
+// pyrDown tile: output rows [oy0, oy0 + kDownRows), output pixels [ox0, ox0 + twp).
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_pyr_down(const uint8_t *__restrict__ src, long long sstride, int sw, int sh,
+                                                       uint8_t *__restrict__ dst, long long dstride, int dw, int dh,
+                                                       int cn, int twp, int border) {
+  using A = typename PyrAcc<T>::A;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  A *V = reinterpret_cast<A *>(smem_raw);
+  const int ox0 = blockIdx.x * twp;
+  const int oy0 = blockIdx.y * kDownRows;
+  const int npx = min(twp, dw - ox0);
+  const int nrows = min(kDownRows, dh - oy0);
+  const int spx = 2 * npx + 3;  // source pixels 2*ox0-2 .. 2*(ox0+npx-1)+2
+  const int span = spx * cn;
+  // Phase 1: vertical sums, V[r * span + e].
+  for (int e = threadIdx.x; e < span; e += kThreads) {
+    const int px = 2 * ox0 - 2 + e / cn;
+    const int ch = e - (e / cn) * cn;
+    const int mx = border_map(px, sw, border);
+    const int se = mx * cn + ch;
+    int ys[5];
+    for (int j = 0; j < 4; j++) ys[j] = border_map(2 * oy0 - 2 + j, sh, border);
+    A r0 = ld<T>(src, sstride, ys[0], se), r1 = ld<T>(src, sstride, ys[1], se);
+    A r2 = ld<T>(src, sstride, ys[2], se), r3 = ld<T>(src, sstride, ys[3], se);
+    for (int r = 0; r < nrows; r++) {
+      const int yb = 2 * (oy0 + r) - 2;
+      const A r4 = ld<T>(src, sstride, border_map(yb + 4, sh, border), se);
+      V[r * span + e] = tap5(r0, r1, r2, r3, r4);
+      const A r5 = r + 1 < nrows ? ld<T>(src, sstride, border_map(yb + 5, sh, border), se) : r4;
+      r0 = r2;
+      r1 = r3;
+      r2 = r4;
+      r3 = r5;
+    }
+  }
+  __syncthreads();
+  // Phase 2: output element j of the tile row sits over padded element 2j - j % cn + 2cn.
+  const int ne = npx * cn;
+  for (int idx = threadIdx.x; idx < nrows * ne; idx += kThreads) {
+    const int r = idx / ne;
+    const int j = idx - r * ne;
+    const int c = 2 * j - j % cn + 2 * cn;
+    const A *v = V + r * span + c;
+    const A s = tap5(v[-2 * cn], v[-cn], v[0], v[cn], v[2 * cn]);
+    reinterpret_cast<T *>(dst + (long long)(oy0 + r) * dstride)[(long long)ox0 * cn + j] = pyr_finish<T, 8>(s);
+  }
+}
+
+// pyrDown for any channel count: one output element per thread, 25 loads.
+template <class T>
+__global__ void k_pyr_down_direct(const uint8_t *__restrict__ src, long long sstride, int sw, int sh,
+                                  uint8_t *__restrict__ dst, long long dstride, int dw, int dh, int cn, int border) {
+  using A = typename PyrAcc<T>::A;
+  const long long ne = (long long)dw * cn;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < ne * dh; i += (long long)gridDim.x * blockDim.x) {
+    const int y = (int)(i / ne);
+    const int j = (int)(i - (long long)y * ne);
+    const int x = j / cn, ch = j - x * cn;
+    A p[5];
+    for (int t = 0; t < 5; t++) {
+      const int se = border_map(2 * x + t - 2, sw, border) * cn + ch;
+      A r[5];
+      for (int k = 0; k < 5; k++) r[k] = ld<T>(src, sstride, border_map(2 * y + k - 2, sh, border), se);
+      p[t] = tap5(r[0], r[1], r[2], r[3], r[4]);
+    }
+    reinterpret_cast<T *>(dst + (long long)y * dstride)[j] = pyr_finish<T, 8>(tap5(p[0], p[1], p[2], p[3], p[4]));
+  }
+}
+
+constexpr int kUpRows = 8;  // source rows per tile (16 output rows)
+
+__device__ __forceinline__ int up_row(int y, int h) { return y < 0 ? (h > 1 ? 1 : 0) : y >= h ? h - 1 : y; }
+
+// pyrUp tile: source rows [sy0, sy0 + kUpRows), source pixels [sx0, sx0 + twp).
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_pyr_up(const uint8_t *__restrict__ src, long long sstride, int sw, int sh,
+                                                     uint8_t *__restrict__ dst, long long dstride, int cn, int twp) {
+  using A = typename PyrAcc<T>::A;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int sx0 = blockIdx.x * twp;
+  const int sy0 = blockIdx.y * kUpRows;
+  const int npx = min(twp, sw - sx0);
+  const int nrows = min(kUpRows, sh - sy0);
+  const int span = (npx + 2) * cn;  // source pixels sx0-1 .. sx0+npx
+  A *E = reinterpret_cast<A *>(smem_raw);
+  A *O = E + kUpRows * span;
+  for (int e = threadIdx.x; e < span; e += kThreads) {
+    const int px = sx0 - 1 + e / cn;
+    const int ch = e - (e / cn) * cn;
+    const int mx = px < 0 ? (sw > 1 ? 1 : 0) : px >= sw ? sw - 1 : px;
+    const int se = mx * cn + ch;
+    A a = ld<T>(src, sstride, up_row(sy0 - 1, sh), se);
+    A b = ld<T>(src, sstride, sy0, se);
+    for (int r = 0; r < nrows; r++) {
+      const A c = ld<T>(src, sstride, up_row(sy0 + r + 1, sh), se);
+      E[r * span + e] = up_even(a, b, c);
+      O[r * span + e] = up_odd(b, c);
+      a = b;
+      b = c;
+    }
+  }
+  __syncthreads();
+  // Output pixel 2p (+1) of tile row r; q[p] is smem element (p - sx0 + 1) * cn.
+  const int ne = 2 * npx * cn;
+  for (int idx = threadIdx.x; idx < 2 * nrows * ne; idx += kThreads) {
+    const int rr = idx / ne;  // output row within the tile
+    const int j = idx - rr * ne;
+    const int opx = j / cn, ch = j - opx * cn;
+    const int p = opx >> 1;
+    const A *q = ((rr & 1) ? O : E) + (rr >> 1) * span + (p + 1) * cn + ch;
+    const A s = (opx & 1) ? up_odd(q[0], q[cn]) : up_even(q[-cn], q[0], q[cn]);
+    reinterpret_cast<T *>(dst + (long long)(2 * sy0 + rr) * dstride)[(long long)2 * sx0 * cn + j] = pyr_finish<T, 6>(s);
+  }
+}
+
+template <class T>
+__global__ void k_pyr_up_direct(const uint8_t *__restrict__ src, long long sstride, int sw, int sh,
+                                uint8_t *__restrict__ dst, long long dstride, int cn) {
+  using A = typename PyrAcc<T>::A;
+  const long long ne = 2LL * sw * cn;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < ne * 2 * sh; i += (long long)gridDim.x * blockDim.x) {
+    const int oy = (int)(i / ne);
+    const int j = (int)(i - (long long)oy * ne);
+    const int opx = j / cn, ch = j - opx * cn;
+    const int y = oy >> 1, p = opx >> 1;
+    auto col = [&](int px) -> A {
+      const int mx = px < 0 ? (sw > 1 ? 1 : 0) : px >= sw ? sw - 1 : px;
+      const int se = mx * cn + ch;
+      const A a = ld<T>(src, sstride, up_row(y - 1, sh), se);
+      const A b = ld<T>(src, sstride, y, se);
+      const A c = ld<T>(src, sstride, up_row(y + 1, sh), se);
+      return (oy & 1) ? up_odd(b, c) : up_even(a, b, c);
+    };
+    const A s = (opx & 1) ? up_odd(col(p), col(p + 1)) : up_even(col(p - 1), col(p), col(p + 1));
+    reinterpret_cast<T *>(dst + (long long)oy * dstride)[j] = pyr_finish<T, 6>(s);
+  }
+}
+
+template <class T>
+cudaError_t pyr_down_t(const DImg &s, const DImg &d, int border, cudaStream_t st) {
+  using A = typename PyrAcc<T>::A;
+  note_launch();
+  if (s.cn > 16) {
+    const long long n = (long long)d.w * d.cn * d.h;
+    const int blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 64);
+    k_pyr_down_direct<T><<<blocks, 256, 0, st>>>(s.p, s.stride, s.w, s.h, d.p, d.stride, d.w, d.h, s.cn, border);
+    return cudaGetLastError();
+  }
+  const int twp = std::max(1, kDownElems / s.cn);
+  const size_t smem = (size_t)kDownRows * (2 * twp + 3) * s.cn * sizeof(A);
+  dim3 grid((d.w + twp - 1) / twp, (d.h + kDownRows - 1) / kDownRows);
+  k_pyr_down<T><<<grid, kThreads, smem, st>>>(s.p, s.stride, s.w, s.h, d.p, d.stride, d.w, d.h, s.cn, twp, border);
+  return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t pyr_up_t(const DImg &s, const DImg &d, cudaStream_t st) {
+  using A = typename PyrAcc<T>::A;
+  note_launch();
+  if (s.cn > 16) {
+    const long long n = (long long)d.w * d.cn * d.h;
+    const int blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 64);
+    k_pyr_up_direct<T><<<blocks, 256, 0, st>>>(s.p, s.stride, s.w, s.h, d.p, d.stride, s.cn);
+    return cudaGetLastError();
+  }
+  const int twp = std::max(1, 128 / s.cn);
+  const size_t smem = (size_t)2 * kUpRows * (twp + 2) * s.cn * sizeof(A);
+  dim3 grid((s.w + twp - 1) / twp, (s.h + kUpRows - 1) / kUpRows);
+  k_pyr_up<T><<<grid, kThreads, smem, st>>>(s.p, s.stride, s.w, s.h, d.p, d.stride, s.cn, twp);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_pyr_down(const DImg &s, const DImg &d, int depth, int border, cudaStream_t st) {
+  switch (depth) {
+    case k8U: return pyr_down_t<uint8_t>(s, d, border, st);
+    case k16U: return pyr_down_t<uint16_t>(s, d, border, st);
+    case k16S: return pyr_down_t<int16_t>(s, d, border, st);
+    case k32F: return pyr_down_t<float>(s, d, border, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_pyr_up(const DImg &s, const DImg &d, int depth, cudaStream_t st) {
+  switch (depth) {
+    case k8U: return pyr_up_t<uint8_t>(s, d, st);
+    case k16U: return pyr_up_t<uint16_t>(s, d, st);
+    case k16S: return pyr_up_t<int16_t>(s, d, st);
+    case k32F: return pyr_up_t<float>(s, d, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace vb

@@ -107,6 +107,31 @@ cudaError_t launch_sub_sat(const DImg &a, const DImg &b, const DImg &d, int dept
 cudaError_t launch_morph_fast(const DImg &s, const DImg &d, bool is_max, const std::vector<uint8_t> &mask, int kw, int kh,
                               cudaStream_t st);
 
+// ------------------------------------------------ fused gray + shrink
+// grayDownsample (src/videoio/frame.zig:169-335): BGR / BGRA u8 -> gray
+// shrunk by the integer factor k (1-16); d is (s.w / k) x (s.h / k).
+cudaError_t launch_gray_downsample(const DImg &s, const DImg &d, int k, cudaStream_t st);
+
+// ------------------------------------------------------------ pyramids
+// pyrDown (src/imgproc/pyramid.zig:73-96): d is ((w+1)/2, (h+1)/2); any border
+// but constant. pyrUp (:408-426): d is (2w, 2h), reflect101 only.
+cudaError_t launch_pyr_down(const DImg &s, const DImg &d, int depth, int border, cudaStream_t st);
+cudaError_t launch_pyr_up(const DImg &s, const DImg &d, int depth, cudaStream_t st);
+
+// ------------------------------------------------- undistort and remap
+// src/calib3d/undistort.zig. Parameter blocks are built on the host into
+// byte vectors (one per stripe of undistort's rows, or one for the map) and
+// passed as device copies (undistort) or by value (the map).
+int undistort_stripe_rows(int width, int height);
+// Returns true when some stripe's camera matrix is singular (its rows are left as they are).
+bool undistort_stripes(const double K[9], const double k8[8], const double *new_k, int width, int height,
+                       std::vector<uint8_t> &out);
+bool undistort_map_params(const double K[9], const double k8[8], const double *R, const double *new_k,
+                          std::vector<uint8_t> &out);
+cudaError_t launch_undistort(const DImg &s, const DImg &d, const void *stripes_dev, cudaStream_t st);
+cudaError_t launch_init_undistort_map(const std::vector<uint8_t> &params, const DImg &mx, const DImg &my, cudaStream_t st);
+cudaError_t launch_remap(const DImg &s, const DImg &d, const DImg &mx, const DImg &my, uint8_t value, cudaStream_t st);
+
 // ------------------------------------------------------- host helpers
 // Gaussian taps (src/imgproc/filter.zig:350-476), in host f64.
 void gaussian_kernel(double *out, int n, double sigma);
