@@ -210,13 +210,15 @@ class Ctx:
 # ----------------------------------------------------------- batched-mixed
 
 N_IMAGES = 256
+IMAGE_LIMIT = 0  # --images: the first N images only (reduced plans for profiling captures)
 E2E_DEPTH = 2  # plans in flight in the end-to-end measurement
 MIX_SEED = 2
 
 
 def mixed_shapes():
     synth = load_synth()
-    return synth.mixed_shapes(N_IMAGES, seed=MIX_SEED)
+    shapes = synth.mixed_shapes(N_IMAGES, seed=MIX_SEED)
+    return shapes[:IMAGE_LIMIT] if IMAGE_LIMIT else shapes
 
 
 def c2_stages(B):
@@ -467,7 +469,7 @@ def bench_batched(args, ctx):
         "metric": METRIC, "value": value, "unit": "Gpix/s", "n_gpus": ctx.world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u8", "data": "synthetic",
-        "config": {"workload": "batched-mixed", "images": N_IMAGES, "shapes": "w U[64,4096], h U[64,2160], 1|3 ch",
+        "config": {"workload": "batched-mixed", "images": len(shapes), "shapes": "w U[64,4096], h U[64,2160], 1|3 ch",
                    "stages": ["gray", "gaussian 5x5", "open 5x5 ellipse", "resize linear 0.5x"],
                    "pixels_per_step": px_step, "bytes_per_step": info["bytes_moved"],
                    "pipeline_gbs": pipeline_gbs, "pipeline_frac": pipeline_gbs / peak,
@@ -1405,7 +1407,11 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="built-in launch defaults instead of the tuned table")
     ap.add_argument("--tuning", default=None, help="tuned table to load, or to write when it was made elsewhere")
     ap.add_argument("--duration", type=float, default=20.0, help="seconds per arrival rate (served workload)")
+    ap.add_argument("--images", type=int, default=0,
+                    help="batched-mixed: the first N images only (a reduced plan for profiler captures; not a bench line)")
     args = ap.parse_args()
+    global IMAGE_LIMIT
+    IMAGE_LIMIT = max(0, args.images)
     ours, ref = WORKLOADS[args.workload]
     subs = args.workload == "batched-mixed" and not args.only and args.gpus == 1
     if args.impl == "reference":

@@ -488,7 +488,9 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
         if (strip_ok && strip_halo(prof, im.v.cn, true) <= 8 && (op == 2 || op == 3) && it == 1) {
           mode[i] = 2;
           Launch *l = class_of(ls, kOpMorphStrip, k8U, im.v.cn, kh, op == 3, true, prof);
-          add_img(l, bimg(im.v, next[i].v), im.input);
+          BImg b = bimg(im.v, next[i].v);
+          b.pad = (im.padded && im.input < 0 ? 1 : 0) | (next[i].padded ? 2 : 0);
+          add_img(l, b, im.input);
           u8_bytes(*l, im.v, next[i].v, 1);
           continue;
         }
@@ -517,6 +519,7 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
           const Buf &im = src[i];
           const DImg from = p == 0 ? im.v : tmp[i][(p - 1) % 2].v;
           const DImg dst = p + 1 == np ? next[i].v : tmp[i][p % 2].v;
+          const bool from_pad = p == 0 ? im.padded && im.input < 0 : true;
           Launch *l;
           if (mode[i] == 1) {
             l = class_of(pl, kOpMorphStrip, k8U, im.v.cn, kh, passes[p], false, prof);
@@ -526,7 +529,9 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
             l = class_of(pl, kOpMorph, k8U, im.v.cn, kh, passes[p]);
             fast::morph_fast_args(mask, kw, kh, im.v.cn, im.v.w, l->ma);
           }
-          add_img(l, bimg(from, dst), p == 0 ? im.input : -1);
+          BImg b = bimg(from, dst);
+          b.pad = (from_pad ? 1 : 0) | 2;
+          add_img(l, b, p == 0 ? im.input : -1);
           u8_bytes(*l, from, dst, depth_size(im.depth));
         }
         for (Launch &l : pl) {

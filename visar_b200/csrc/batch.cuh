@@ -32,6 +32,7 @@ struct BImg {
   float cv;             // border value as f32
   int wide;             // source rows allow 8-byte loads
   int lanes;            // row-tiled operations: log2 of the threads per row
+  int pad;              // warp strips: bit 0 source, bit 1 destination rows padded to 8-sample words
 };
 
 struct TileQ {
@@ -728,7 +729,7 @@ struct OpMorphStrip {
   using Args = NoArgs;
   static size_t smem(const Args &) { return 0; }
   static __device__ __forceinline__ void tile(const BImg &im, const Args &, int tx, int ty, int lane) {
-    strip::MorphStrip<P1, P2, CN, RH, MAX1, FUSED>::run(im.s, im.d, tx, ty, lane);
+    strip::MorphStrip<P1, P2, CN, RH, MAX1, FUSED>::run(im.s, im.d, im.pad, tx, ty, lane);
   }
 };
 

@@ -17,6 +17,9 @@ struct Buf {
   DImg v;
   int depth;
   int input = -1;  // index of the plan input this buffer is, else -1
+  // Engine-owned pitched image: every row can be read and written up to its
+  // pitch (at least its length rounded up to 8 samples).
+  bool padded = false;
 };
 
 enum OpKind {
@@ -179,6 +182,7 @@ struct Builder {
     void *p = take(pitch * (size_t)h);
     if (!sizing && !p) return false;
     out = Buf{DImg{static_cast<uint8_t *>(p), (long long)pitch, w, h, cn}, depth};
+    out.padded = true;
     return true;
   }
   template <class T>

@@ -21,8 +21,9 @@
 // Rows stream through a per-lane queue in shared memory: the copy of row
 // j + kQD (cp.async) is issued when row j is computed, so kQD rows per lane
 // are always in flight. State that moves down with the rows (the Gaussian
-// cascade, the morphology accumulators) alternates between register sets
-// across an unrolled row loop instead of being moved.
+// cascade, the morphology row windows) alternates between register sets or
+// rotates through compile-time ring slots across an unrolled row loop
+// instead of being moved.
 #pragma once
 #include <utility>
 #include "morphfast.cuh"
@@ -400,58 +401,104 @@ template <bool MAX>
 __device__ __forceinline__ uint32_t pop(uint32_t a, uint32_t b) {
   return MAX ? __vmaxu2(a, b) : __vminu2(a, b);
 }
+// Three-input min / max on 16-bit lanes: one instruction, the cost of pop.
+template <bool MAX>
+__device__ __forceinline__ uint32_t pop3(uint32_t a, uint32_t b, uint32_t c) {
+  return MAX ? __vimax3_u16x2(a, b, c) : __vimin3_u16x2(a, b, c);
+}
 
-// Runs of every half-width 0..M over this lane's four pairs.
-template <int M, int CN, bool MAX>
-__device__ __forceinline__ void pair_runs(const uint32_t (&own)[4], uint32_t (&r)[M + 1][4]) {
-  constexpr int REACH = M * CN;
+// Band decomposition of an element whose rows are centred runs, symmetric
+// about the centre row, with half-widths that never grow away from it
+// (every rect / cross / ellipse of getStructuringElement). With d(a) the
+// half-width of the rows at distance a from the centre, the element is the
+// union over a of the centred rectangles (2 d(a) + 1) x (2 a + 1), so
+//   extremum over the element = extremum over a of H_d(a)(V_a)
+// where V_a is the vertical extremum over the rows within distance a and H_d
+// the horizontal run of half-width d. Only the a where the half-width drops
+// next (or a = AY) are needed; rows whose half-width is 0 fold into the
+// result directly.
+template <class PR>
+struct Bands {
+  static constexpr int KH = PR::KH, AY = KH / 2;
+  __host__ __device__ static constexpr int d(int a) { return PR::at(AY + a); }
+  __host__ __device__ static constexpr bool part(int a) { return a == AY || d(a) > d(a + 1); }
+  // The last part with a horizontal run (d > 0), -1 if none.
+  __host__ __device__ static constexpr int last_wide() {
+    int l = -1;
+    for (int a = 0; a <= AY; a++)
+      if (part(a) && d(a) > 0) l = a;
+    return l;
+  }
+  __host__ __device__ static constexpr bool valid() {
+    if (KH % 2 == 0) return false;
+    for (int i = 0; i < KH; i++)
+      if (PR::at(i) != PR::at(KH - 1 - i) || PR::at(i) < 0) return false;
+    for (int a = 1; a <= AY; a++)
+      if (d(a) > d(a - 1)) return false;
+    return true;
+  }
+};
+
+// Horizontal run of half-width D over the four pairs v of every lane.
+template <int D, int CN, bool MAX>
+__device__ __forceinline__ void hrun(const uint32_t (&v)[4], uint32_t (&r)[4]) {
+  constexpr int REACH = D * CN;
   constexpr int NL = (REACH + kSPL - 1) / kSPL;
   Window<NL, -REACH, kSPL - 1 + REACH> win;
-  win.gather(own);
+  win.gather(v);
 #pragma unroll
   for (int p = 0; p < 4; p++) {
-    const int o = 2 * p;
-    r[0][p] = own[p];
+    r[p] = v[p];
 #pragma unroll
-    for (int w = 1; w <= M; w++) r[w][p] = pop<MAX>(r[w - 1][p], pop<MAX>(win.at(o - w * CN), win.at(o + w * CN)));
+    for (int w = 1; w <= D; w++) r[p] = pop3<MAX>(r[p], win.at(2 * p - w * CN), win.at(2 * p + w * CN));
   }
 }
 
-// Running vertical combination: logical accumulator j collects the output
-// row that element row j of the current source row contributes to; after
-// each source row the last one is complete and the others move up by one.
-// The accumulators form a ring: at phase PH (source rows added so far, mod
-// KH) logical j lives in slot (j - PH) mod KH, so with the row loop unrolled
-// by KH every slot index is a compile-time constant and nothing moves.
-template <class PR, bool MAX>
-struct Ring {
-  static constexpr int KH = PR::KH;
-  static constexpr uint32_t I = MAX ? 0u : 0x00FF00FFu;
-  uint32_t a[KH][4];
-  __device__ __forceinline__ void init() {
+// Band a of the decomposition (ascending): V grows to the rows within
+// distance A, and a part with a horizontal run adds H_d(A)(V) to out (HAVE:
+// out already holds a part).
+template <class PR, int CN, bool MAX, int ROT, int A, bool HAVE>
+struct BandStep {
+  static __device__ __forceinline__ void run(const uint32_t (&h)[PR::KH][4], uint32_t (&V)[4], uint32_t (&out)[4]) {
+    using B = Bands<PR>;
+    constexpr int KH = B::KH, AY = B::AY, LW = B::last_wide();
+    if constexpr (A > 0) {
 #pragma unroll
-    for (int j = 0; j < KH; j++)
-#pragma unroll
-      for (int p = 0; p < 4; p++) a[j][p] = I;
-  }
-  // Adds a row of runs at phase PH; o receives the completed output row.
-  template <int PH, int M>
-  __device__ __forceinline__ void add(const uint32_t (&r)[M + 1][4], uint32_t (&o)[4]) {
-#pragma unroll
-    for (int j = 0; j < KH; j++) {
-      const int sl = (j + KH - PH) % KH;
-      const int dj = PR::at(j);
-#pragma unroll
-      for (int p = 0; p < 4; p++) {
-        if (j == 0) a[sl][p] = dj < 0 ? I : r[dj][p];  // a fresh accumulator
-        else if (dj >= 0) a[sl][p] = pop<MAX>(a[sl][p], r[dj][p]);
-      }
+      for (int p = 0; p < 4; p++) V[p] = pop3<MAX>(V[p], h[(ROT + AY - A) % KH][p], h[(ROT + AY + A) % KH][p]);
     }
-    constexpr int last = (KH - 1 + KH - PH) % KH;
+    constexpr bool PART = B::part(A) && B::d(A) > 0;
+    if constexpr (PART) {
+      uint32_t P[4];
+      hrun<B::d(A), CN, MAX>(V, P);
 #pragma unroll
-    for (int p = 0; p < 4; p++) o[p] = a[last][p];
+      for (int p = 0; p < 4; p++) out[p] = HAVE ? pop<MAX>(out[p], P[p]) : P[p];
+    }
+    if constexpr (A < LW) BandStep<PR, CN, MAX, ROT, A + 1, HAVE || PART>::run(h, V, out);
   }
 };
+
+// The extremum over element PR of the KH rows in h, row i (of the window
+// centred on the output row) in slot (ROT + i) % KH.
+template <class PR, int CN, bool MAX, int ROT>
+__device__ __forceinline__ void band_apply(const uint32_t (&h)[PR::KH][4], uint32_t (&out)[4]) {
+  using B = Bands<PR>;
+  static_assert(B::valid(), "band decomposition needs a symmetric element narrowing away from its centre");
+  constexpr int KH = B::KH, AY = B::AY, LW = B::last_wide();
+  uint32_t V[4];
+#pragma unroll
+  for (int p = 0; p < 4; p++) V[p] = h[(ROT + AY) % KH][p];
+  if constexpr (LW >= 0) {
+    BandStep<PR, CN, MAX, ROT, 0, false>::run(h, V, out);
+  } else {
+#pragma unroll
+    for (int p = 0; p < 4; p++) out[p] = V[p];
+  }
+  // Rows beyond the last run have half-width 0: their centre samples.
+#pragma unroll
+  for (int a = (LW < 0 ? 1 : LW + 1); a <= AY; a++)
+#pragma unroll
+    for (int p = 0; p < 4; p++) out[p] = pop3<MAX>(out[p], h[(ROT + AY - a) % KH][p], h[(ROT + AY + a) % KH][p]);
+}
 
 // Pair lanes of samples outside the row set to the identity.
 __device__ __forceinline__ void mask_pairs(uint32_t (&v)[4], const Cols &c, uint32_t ident) {
@@ -471,8 +518,10 @@ __device__ __forceinline__ void mask_pairs(uint32_t (&v)[4], const Cols &c, uint
 // strip whose outer HALO lanes are not written. A lane's first-pass value at
 // a sample is exact once the samples within its reach exist in the strip, so
 // HALO lanes covering (M1 + M2) * CN samples suffice. Source rows come
-// through the shared-memory row queue; the row loop is unrolled by the
-// element height (ring accumulators).
+// through the shared-memory row queue. The last KH rows of each pass's input
+// stay in a register ring (row t in slot t mod KH; the row loop is unrolled
+// by KH, so every slot index is a compile-time constant and nothing moves),
+// and each output row is the band decomposition of its KH input rows.
 template <class P1, class P2, int CN, int RH, bool MAX1, bool FUSED>
 struct MorphStrip {
   static constexpr int M1 = P1::maxd(), M2 = FUSED ? P2::maxd() : 0;
@@ -484,16 +533,22 @@ struct MorphStrip {
   static constexpr int NSRC = RH + (KH1 - 1) + (FUSED ? KH2 - 1 : 0);
   static constexpr bool MAX2 = !MAX1;
   static constexpr uint32_t I1 = MAX1 ? 0u : 0xFFFFFFFFu;
+  static constexpr uint32_t I1p = MAX1 ? 0u : 0x00FF00FFu;
   static constexpr uint32_t I2p = MAX2 ? 0u : 0x00FF00FFu;
+  // Tile modes: every lane inside the row; lanes inside, entirely outside
+  // (predicated fills) or straddling the row's end with an 8-byte copy into
+  // the row padding (masked per pair); any other tile (per-sample paths).
+  enum Mode { kInside, kEdge, kSlow };
 
   const DImg s, d;  // copies (kept in registers across the row loop)
   long long n, gs;
   int H, first, nsrc, ylim;
-  bool out_lane;
+  bool out_lane, live;
   Cols c;
   RowQueue q;
-  Ring<P1, MAX1> acc1;
-  Ring<P2, MAX2> acc2;
+  uint32_t keep[4];     // kEdge: 16-bit lanes of samples inside the row
+  uint32_t h1[KH1][4];  // the first pass's input rows
+  uint32_t h2[KH2][4];  // the second pass's input rows (first-pass results)
 
   __device__ __forceinline__ MorphStrip(const DImg &s_, const DImg &d_, int tx, int ty, int lane) : s(s_), d(d_) {
     n = (long long)s.w * CN;
@@ -506,89 +561,104 @@ struct MorphStrip {
     ylim = min(y0 + RH, d.h);
     nsrc = min(NSRC, ylim - y0 + KH1 + KH2 - 2);
     out_lane = lane >= HALO && lane < 32 - HALO && gs < n;
+    live = gs < n && gs + kSPL > 0;
     q = row_queue(lane);
   }
 
   // Source row j into its slot (rows j >= nsrc: nothing is read).
-  template <bool INSIDE>
+  template <int MODE>
   __device__ __forceinline__ void fetch(int j) {
     const int sy = first + j;
     const bool in = sy >= 0 && sy < H;
-    if constexpr (INSIDE) {
+    if constexpr (MODE == kInside) {
       fetch8_inside(q.slot(j), row_ptr<const uint8_t>(s, in ? sy : 0) + gs, in && j < nsrc, I1);
+    } else if constexpr (MODE == kEdge) {
+      fetch8_inside(q.slot(j), row_ptr<const uint8_t>(s, in ? sy : 0) + gs, in && j < nsrc && live, I1);
     } else {
       if (j < nsrc) fetch8(q.slot(j), in ? row_ptr<const uint8_t>(s, sy) : nullptr, c, I1);
     }
   }
 
   // Output row y, written when it belongs to the tile and the image.
-  template <bool INSIDE>
+  template <int MODE>
   __device__ __forceinline__ void put(int y, const uint32_t (&o)[4]) {
     const uint2 o8 = pack_pairs(o);
     const bool ok = out_lane && y < ylim;
-    if constexpr (INSIDE) {
+    if constexpr (MODE != kSlow) {
       st_global8_if(row_ptr<uint8_t>(d, ok ? y : 0) + gs, o8, ok);
     } else {
       if (ok) store8(row_ptr<uint8_t>(d, y), gs, n, o8.x, o8.y);
     }
   }
 
-  // Source row j; PH = j mod KH1 (the accumulators' phase). Rows past nsrc
-  // (the last group of KH1) compute values that are not stored.
-  template <bool INSIDE, int PH>
+  // Source row j; PH = j mod KH1. Rows past nsrc (the last group of KH1)
+  // compute values that are not stored.
+  template <int MODE, int PH>
   __device__ __forceinline__ void step(int j) {
     cp_wait<kQD - 1>();  // row j has landed
     const uint2 cur = ld_shared8(q.slot(j));
-    fetch<INSIDE>(j + kQD);
+    fetch<MODE>(j + kQD);
     cp_commit();
-    uint32_t v[4];
-    unpack_pairs(cur, v);
-    uint32_t r1[M1 + 1][4];
-    pair_runs<M1, CN, MAX1>(v, r1);
-    uint32_t o1[4];
-    acc1.template add<PH, M1>(r1, o1);
+    unpack_pairs(cur, h1[PH]);
+    if constexpr (MODE == kEdge) {
+#pragma unroll
+      for (int p = 0; p < 4; p++) h1[PH][p] = (h1[PH][p] & keep[p]) | (I1p & ~keep[p]);
+    }
     if (j < KH1 - 1) return;
+    uint32_t o1[4];
+    band_apply<P1, CN, MAX1, (PH + 1) % KH1>(h1, o1);
     const int y1 = first + j - (KH1 - 1) + AY1;  // first-pass row completed
     if constexpr (!FUSED) {
-      put<INSIDE>(y1, o1);
+      put<MODE>(y1, o1);
     } else {
-      // First-pass values outside the image are the second pass's identity.
+      // First-pass row t2 = j - (KH1 - 1) goes to slot t2 mod KH2; values
+      // outside the image are the second pass's identity.
+      constexpr int S2 = (PH + 1) % KH2;
       const bool rin = y1 >= 0 && y1 < H;
 #pragma unroll
-      for (int p = 0; p < 4; p++) o1[p] = rin ? o1[p] : I2p;
-      if constexpr (!INSIDE) mask_pairs(o1, c, I2p);
-      uint32_t r2[M2 + 1][4];
-      pair_runs<M2, CN, MAX2>(o1, r2);
-      uint32_t o2[4];
-      // acc2 has taken j - (KH1 - 1) rows before this one.
-      acc2.template add<(PH + 2 * KH2 - (KH1 - 1) % KH2) % KH2, M2>(r2, o2);
+      for (int p = 0; p < 4; p++) {
+        const uint32_t v = rin ? o1[p] : I2p;
+        h2[S2][p] = MODE == kEdge ? (v & keep[p]) | (I2p & ~keep[p]) : v;
+      }
+      if constexpr (MODE == kSlow) mask_pairs(h2[S2], c, I2p);
       if (j < (KH1 - 1) + (KH2 - 1)) return;
-      put<INSIDE>(y1 - (KH2 - 1) + AY2, o2);
+      uint32_t o2[4];
+      band_apply<P2, CN, MAX2, (PH + 2) % KH2>(h2, o2);
+      put<MODE>(y1 - (KH2 - 1) + AY2, o2);
     }
   }
 
-  template <bool INSIDE, int... PH>
+  template <int MODE, int... PH>
   __device__ __forceinline__ void steps(int j, std::integer_sequence<int, PH...>) {
-    (step<INSIDE, PH>(j + PH), ...);
+    (step<MODE, PH>(j + PH), ...);
   }
 
-  template <bool INSIDE>
+  template <int MODE>
   __device__ __forceinline__ void rows() {
-    acc1.init();
-    acc2.init();
+    if constexpr (MODE == kEdge) {
+#pragma unroll
+      for (int p = 0; p < 4; p++) {
+        const long long k = gs + 2 * p;
+        keep[p] = (k >= 0 && k < n ? 0x0000FFFFu : 0u) | (k + 1 >= 0 && k + 1 < n ? 0xFFFF0000u : 0u);
+      }
+    }
 #pragma unroll 1
     for (int j = 0; j < kQD; j++) {
-      fetch<INSIDE>(j);
+      fetch<MODE>(j);
       cp_commit();
     }
 #pragma unroll 1
-    for (int j = 0; j < nsrc; j += KH1) steps<INSIDE>(j, std::make_integer_sequence<int, KH1>{});
+    for (int j = 0; j < nsrc; j += KH1) steps<MODE>(j, std::make_integer_sequence<int, KH1>{});
   }
 
-  static __device__ __forceinline__ void run(const DImg &s, const DImg &d, int tx, int ty, int lane) {
+  // pad: bit 0 = source rows readable, bit 1 = destination rows writable, up
+  // to their length rounded up to 8 samples (the engine's pitched images).
+  static __device__ __forceinline__ void run(const DImg &s, const DImg &d, int pad, int tx, int ty, int lane) {
     MorphStrip m(s, d, tx, ty, lane);
-    if (__all_sync(kFull, m.c.inside)) m.template rows<true>();
-    else m.template rows<false>();
+    const bool straddle = m.live && !m.c.inside;
+    if (__all_sync(kFull, m.c.inside)) m.template rows<kInside>();
+    else if (__all_sync(kFull, !straddle || (pad & 3) == 3)) m.template rows<kEdge>();
+    else m.template rows<kSlow>();
   }
 };
 
