@@ -108,6 +108,28 @@ int visar_init_undistort_rectify_map(const double k[9], const double *dist, size
 int visar_remap(const visar_image *src, const visar_image *dst, const visar_image *mapx, const visar_image *mapy,
                 double value);
 
+/* The tracker's per-frame tail (demos/track_lib.zig:533-553 in VISAR). */
+/* include/visar.h:70, src/capi.zig:326-337 -> src/imgproc/threshold.zig:307-360. 8U one channel;
+   method 0 MEAN_C, 1 GAUSSIAN_C; type 0 BINARY, 1 BINARY_INV; odd block_size >= 3. */
+int visar_adaptive_threshold(const visar_image *src, const visar_image *dst, double maxval, int method, int type,
+                             int block_size, double delta);
+/* include/visar.h:76, src/capi.zig:382-386 -> src/imgproc/hist.zig:22-45. 8U one channel. */
+int visar_equalize_hist(const visar_image *src, const visar_image *dst);
+/* include/visar.h:78, src/capi.zig:529-551 -> src/imgproc/components.zig:408. labels: VISAR_32S image
+   of src's size; connectivity 4 (else 8); stats (may be NULL): up to max rows of left, top, width,
+   height, area; centroids (may be NULL): up to max rows of cx, cy; *count: labels incl. background.
+   stats and centroids are host arrays. */
+int visar_connected_components(const visar_image *src, const visar_image *labels, int connectivity, int32_t *stats,
+                               double *centroids, size_t max, size_t *count);
+/* include/visar.h:191-195, src/capi.zig:446-469 -> src/video/track.zig:17-82. Running-average
+   background (learning rate 1 / 2^shift, shift 0-15): mask (8U, frame size) is 255 where the gray
+   frame differs from the model by more than threshold; the first frame primes the model. The model
+   lives on the device current at create. */
+typedef struct visar_background visar_background;
+int visar_background_create(uint32_t width, uint32_t height, int shift, visar_background **out);
+int visar_background_apply(visar_background *b, const visar_image *frame, const visar_image *mask, int threshold);
+void visar_background_free(visar_background *b);
+
 /* Additive exports (Zig API only in VISAR, no C entry point there). */
 /* src/imgproc/geometry.zig:586-589 warpPerspective(exec, src, dst, [9]f64, WarpInterp, Border, f64) */
 int visar_warp_perspective(const visar_image *src, const visar_image *dst, const double m[9], int interpolation, int border, double value);

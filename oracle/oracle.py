@@ -221,6 +221,57 @@ def remap(a, mapx, mapy, value=0.0, dst=None):
     return dst
 
 
+def equalize_hist(a, dst=None):
+    dst = np.empty_like(a) if dst is None else dst
+    _check(lib.oracle_equalize_hist(ctypes.byref(desc(a)), ctypes.byref(desc(dst))))
+    return dst
+
+
+lib.oracle_adaptive_threshold.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_int, ctypes.c_double]
+
+
+def adaptive_threshold(a, maxval, method, kind, block, delta, dst=None):
+    dst = np.empty_like(a) if dst is None else dst
+    _check(lib.oracle_adaptive_threshold(ctypes.byref(desc(a)), ctypes.byref(desc(dst)), maxval, method, kind, block, delta))
+    return dst
+
+
+class Background:
+    """The running-average background model (track.zig:17-82) on the host."""
+
+    def __init__(self, w, h, shift):
+        self.model = np.zeros((h, w), np.uint16)
+        self.primed = ctypes.c_int(0)
+        self.shift = shift
+
+    def apply(self, frame, threshold, mask=None):
+        mask = np.empty_like(frame) if mask is None else mask
+        _check(lib.oracle_background_apply(self.model.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16)),
+                                           ctypes.byref(self.primed), self.shift, ctypes.byref(desc(frame)),
+                                           ctypes.byref(desc(mask)), int(threshold)))
+        return mask
+
+
+lib.oracle_connected_components.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                            ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_double),
+                                            ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]
+
+
+def connected_components(a, connectivity=8, max_stats=None):
+    """(count, labels int32, stats (count x 5), centroids (count x 2))."""
+    labels = np.empty(a.shape[:2], np.int32)
+    cap = max_stats if max_stats is not None else a.shape[0] * a.shape[1] + 1
+    stats = np.zeros((cap, 5), np.int32)
+    cents = np.zeros((cap, 2), np.float64)
+    n = ctypes.c_size_t(0)
+    _check(lib.oracle_connected_components(ctypes.byref(desc(a)), ctypes.byref(desc(labels)), int(connectivity),
+                                           stats.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                           cents.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), cap, ctypes.byref(n)))
+    k = min(n.value, cap)
+    return n.value, labels, stats[:k], cents[:k]
+
+
 def morphology(a, op, shape, ksize, iterations=1, dst=None):
     dst = np.empty_like(a) if dst is None else dst
     _check(lib.oracle_morphology(ctypes.byref(desc(a)), ctypes.byref(desc(dst)), op, shape, ksize[0], ksize[1], iterations))

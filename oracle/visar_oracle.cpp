@@ -1871,6 +1871,86 @@ void sample_fixed(const Img<uint8_t> &s, int iu, int iv, uint8_t *o) {
   }
 }
 
+// ================================================== tracker tail (f4)
+
+// equalizeHist (src/imgproc/hist.zig:20-45): LUT from the cumulative
+// histogram without the first occupied bin, f32 scale, sat.cast.
+void equalize_lut(const uint32_t hist[256], uint64_t total, uint8_t lut[256], bool &fill, int &fill_value) {
+  int i = 0;
+  while (hist[i] == 0) i++;
+  fill = hist[i] == total;
+  fill_value = i;
+  for (int k = 0; k < 256; k++) lut[k] = 0;
+  if (fill) return;
+  const float scale = 255.0f / (float)(total - hist[i]);
+  uint32_t acc = 0;
+  lut[i] = 0;
+  for (int k = i + 1; k < 256; k++) {
+    acc += hist[k];
+    lut[k] = cast<uint8_t>((float)acc * scale);
+  }
+}
+
+// connectedComponentsWithStats (src/imgproc/components.zig) by flood fill
+// with OpenCV's numbering, as VISAR's own test reference (components.zig:562-
+// 613): components in raster order of their first pixel (4-connectivity) or
+// of their first 2x2 block (8-connectivity); statistics from integer sums.
+struct CcStat {
+  long long x0, y0, x1, y1, area, sx2, sy;
+};
+
+int cc_label(const Img<uint8_t> &s, std::vector<int32_t> &out, int conn, std::vector<CcStat> &st) {
+  const int w = s.w, h = s.h;
+  out.assign((size_t)w * h, 0);
+  std::vector<std::pair<int, int>> stack;
+  int next = 1;
+  auto flood = [&](int x, int y, int l) {
+    out[(size_t)y * w + x] = l;
+    stack.push_back({x, y});
+    while (!stack.empty()) {
+      const auto p = stack.back();
+      stack.pop_back();
+      for (int dy = -1; dy <= 1; dy++)
+        for (int dx = -1; dx <= 1; dx++) {
+          if ((dx == 0 && dy == 0) || (conn == 4 && dx != 0 && dy != 0)) continue;
+          const int nx = p.first + dx, ny = p.second + dy;
+          if (nx < 0 || ny < 0 || nx >= w || ny >= h) continue;
+          if (s.row(ny)[nx] == 0 || out[(size_t)ny * w + nx] != 0) continue;
+          out[(size_t)ny * w + nx] = l;
+          stack.push_back({nx, ny});
+        }
+    }
+  };
+  if (conn == 4) {
+    for (int y = 0; y < h; y++)
+      for (int x = 0; x < w; x++)
+        if (s.row(y)[x] != 0 && out[(size_t)y * w + x] == 0) flood(x, y, next++);
+  } else {
+    for (int by = 0; by < (h + 1) / 2; by++)
+      for (int bx = 0; bx < (w + 1) / 2; bx++)
+        for (int dy = 0; dy < 2; dy++)
+          for (int dx = 0; dx < 2; dx++) {
+            const int x = bx * 2 + dx, y = by * 2 + dy;
+            if (x >= w || y >= h || s.row(y)[x] == 0 || out[(size_t)y * w + x] != 0) continue;
+            flood(x, y, next++);
+          }
+  }
+  const long long big = std::numeric_limits<long long>::max();
+  st.assign(next, CcStat{big, big, 0, 0, 0, 0, 0});
+  for (int y = 0; y < h; y++)
+    for (int x = 0; x < w; x++) {
+      CcStat &a = st[out[(size_t)y * w + x]];
+      a.x0 = std::min<long long>(a.x0, x);
+      a.y0 = std::min<long long>(a.y0, y);
+      a.x1 = std::max<long long>(a.x1, x);
+      a.y1 = std::max<long long>(a.y1, y);
+      a.area++;
+      a.sx2 += 2LL * x;
+      a.sy += y;
+    }
+  return next;
+}
+
 // ============================================================== dispatch
 
 int src_depth(const visar_image *c) {
@@ -2171,6 +2251,122 @@ int oracle_remap(const visar_image *src, const visar_image *dst, const visar_ima
         }
       }
     });
+  });
+}
+
+int oracle_equalize_hist(const visar_image *src, const visar_image *dst) {
+  return guarded([&] {
+    Img<uint8_t> s = typed<uint8_t>(src, 0);
+    Img<uint8_t> d = typed<uint8_t>(dst, 0);
+    if (s.cn != 1 || s.w != d.w || s.h != d.h || s.cn != d.cn) fail(VISAR_SIZE_MISMATCH, "SizeMismatch");
+    uint32_t hist[256] = {0};
+    for (int y = 0; y < s.h; y++)
+      for (int x = 0; x < s.w; x++) hist[s.row(y)[x]]++;
+    uint8_t lut[256];
+    bool fill;
+    int fv;
+    equalize_lut(hist, (uint64_t)s.w * s.h, lut, fill, fv);
+    for (int y = 0; y < s.h; y++)
+      for (int x = 0; x < s.w; x++) d.row(y)[x] = fill ? (uint8_t)fv : lut[s.row(y)[x]];
+  });
+}
+
+// adaptiveThreshold (src/imgproc/threshold.zig:307-360, C ABI capi.zig:326-337).
+int oracle_adaptive_threshold(const visar_image *src, const visar_image *dst, double maxval, int method, int type, int block,
+                              double delta) {
+  return guarded([&] {
+    if (method != 0 && method != 1) fail(VISAR_INVALID_ARGUMENT, "InvalidArgument");
+    if (type != 0 && type != 1) fail(VISAR_INVALID_ARGUMENT, "InvalidArgument");
+    if (block < 3) fail(VISAR_INVALID_ARGUMENT, "InvalidArgument");
+    Img<uint8_t> s = typed<uint8_t>(src, 0);
+    Img<uint8_t> d = typed<uint8_t>(dst, 0);
+    if (s.w != d.w || s.h != d.h || s.cn != d.cn) fail(VISAR_SIZE_MISMATCH, "SizeMismatch");
+    if (s.cn != 1) fail(VISAR_UNSUPPORTED, "UnsupportedChannels");
+    if (block % 2 != 1) fail(VISAR_INVALID_ARGUMENT, "InvalidKernel");
+    std::vector<uint8_t> mbuf((size_t)s.w * s.h);
+    visar_image mi{(uint32_t)s.w, (uint32_t)s.h, 1, 0, (size_t)s.w, mbuf.data()};
+    if (method == 0) {
+      box_t<uint8_t>(src, &mi, 0, block, block, true, 1);
+    } else {
+      std::vector<float> f((size_t)s.w * s.h), fb((size_t)s.w * s.h);
+      for (int y = 0; y < s.h; y++)
+        for (int x = 0; x < s.w; x++) f[(size_t)y * s.w + x] = (float)s.row(y)[x];
+      visar_image fi{(uint32_t)s.w, (uint32_t)s.h, 1, 5, (size_t)s.w * 4, f.data()};
+      visar_image fo{(uint32_t)s.w, (uint32_t)s.h, 1, 5, (size_t)s.w * 4, fb.data()};
+      gaussian_t<float>(&fi, &fo, 5, block, block, 0.0, 0.0, 1);
+      for (size_t i = 0; i < fb.size(); i++) mbuf[i] = cast<uint8_t>(fb[i]);
+    }
+    const int imax = cast<uint8_t>(maxval);
+    double dl = type == 0 ? std::ceil(delta) : std::floor(delta);
+    dl = std::min(std::max(dl, -1024.0), 1024.0);
+    const int idelta = (int)dl;
+    for (int y = 0; y < s.h; y++)
+      for (int x = 0; x < s.w; x++) {
+        const int sv = s.row(y)[x], mv = mbuf[(size_t)y * s.w + x];
+        const bool gt = sv + idelta > mv;
+        d.row(y)[x] = (uint8_t)((type == 0 ? gt : !gt) ? imax : 0);
+      }
+  });
+}
+
+// Background.apply (src/video/track.zig:30-81) on an explicit u16 model.
+int oracle_background_apply(uint16_t *model, int *primed, int shift, const visar_image *frame, const visar_image *mask,
+                            int threshold) {
+  return guarded([&] {
+    Img<uint8_t> f = typed<uint8_t>(frame, 0);
+    Img<uint8_t> m = typed<uint8_t>(mask, 0);
+    if (f.cn != 1 || f.w != m.w || f.h != m.h || f.cn != m.cn) fail(VISAR_SIZE_MISMATCH, "SizeMismatch");
+    const int t = std::min(std::max(threshold, 0), 255);
+    for (int y = 0; y < f.h; y++)
+      for (int x = 0; x < f.w; x++) {
+        uint16_t &b = model[(size_t)y * f.w + x];
+        const int fv = f.row(y)[x];
+        if (!*primed) {
+          b = (uint16_t)(fv << 8);
+          m.row(y)[x] = 0;
+          continue;
+        }
+        const int bv = b;
+        const bool fg = std::abs(fv - (bv >> 8)) > t;
+        m.row(y)[x] = fg ? 255 : 0;
+        const int sh = shift + (fg ? 2 : 0);
+        b = (uint16_t)(bv + (((fv << 8) - bv) >> sh));
+      }
+    *primed = 1;
+  });
+}
+
+// visar_connected_components (capi.zig:529-551): labels, count, stats rows
+// (left, top, width, height, area), centroids (cx, cy).
+int oracle_connected_components(const visar_image *src, const visar_image *labels, int connectivity, int32_t *stats,
+                                double *centroids, size_t max, size_t *count) {
+  return guarded([&] {
+    Img<uint8_t> s = typed<uint8_t>(src, 0);
+    Img<int32_t> l = typed<int32_t>(labels, 4);
+    if (s.cn != 1 || l.cn != 1 || s.w != l.w || s.h != l.h) fail(VISAR_SIZE_MISMATCH, "SizeMismatch");
+    std::vector<int32_t> out;
+    std::vector<CcStat> st;
+    const int n = cc_label(s, out, connectivity == 4 ? 4 : 8, st);
+    for (int y = 0; y < s.h; y++)
+      for (int x = 0; x < s.w; x++) l.row(y)[x] = out[(size_t)y * s.w + x];
+    *count = (size_t)n;
+    for (size_t i = 0; i < std::min<size_t>(max, (size_t)n); i++) {
+      const CcStat &a = st[i];
+      if (stats) {
+        int32_t *o = stats + i * 5;
+        if (a.area == 0) {
+          o[0] = -1; o[1] = std::numeric_limits<int32_t>::max(); o[2] = 0; o[3] = 0; o[4] = 0;
+        } else {
+          o[0] = (int32_t)a.x0; o[1] = (int32_t)a.y0; o[2] = (int32_t)(a.x1 - a.x0 + 1); o[3] = (int32_t)(a.y1 - a.y0 + 1);
+          o[4] = (int32_t)a.area;
+        }
+      }
+      if (centroids) {
+        const double ar = (double)std::max<long long>(a.area, 1);
+        centroids[2 * i] = a.area == 0 ? std::nan("") : (double)a.sx2 / 2.0 / ar;
+        centroids[2 * i + 1] = a.area == 0 ? std::nan("") : (double)a.sy / ar;
+      }
+    }
   });
 }
 

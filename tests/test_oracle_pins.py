@@ -501,3 +501,83 @@ def test_undistort_remap_refusals():
     with pytest.raises(O.OracleError) as e:
         O.remap(img, mx, mx, dst=np.zeros((20, 30), np.uint8))
     assert e.value.status == -3
+
+
+# --------------------------------------------------------------- tracker tail
+
+import pins_tail as PT  # noqa: E402
+
+
+def test_equalize_known_answer_and_cv2():
+    # hist.zig:67-75
+    assert O.equalize_hist(np.array([[10, 10, 20, 30]], np.uint8)).tolist() == [[0, 0, 128, 255]]
+    import cv2
+    rng = np.random.default_rng(3)
+    for img in (natural(120, 160, 1), rng.integers(40, 90, (37, 53), dtype=np.uint8), np.full((5, 7), 9, np.uint8)):
+        assert np.array_equal(O.equalize_hist(img), cv2.equalizeHist(img))
+
+
+@pytest.mark.parametrize("conn", [4, 8])
+def test_connected_components_reference_patterns_and_cv2(conn):
+    # components.zig:545-650 (patterns, sizes) against cv2 4.13's
+    # connectedComponentsWithStats: labels, stats and centroids exactly.
+    import cv2
+    rng = np.random.default_rng(42)
+    for w, h in PT.CC_SIZES:
+        for pat in PT.PATTERNS:
+            img = PT.cc_pattern(w, h, pat, rng)
+            n, lab, st, ce = O.connected_components(img, conn)
+            n2, lab2, st2, ce2 = cv2.connectedComponentsWithStats(img, connectivity=conn, ltype=cv2.CV_32S)
+            assert n == n2 and np.array_equal(lab, lab2) and np.array_equal(st, st2), (w, h, pat)
+            assert np.array_equal(np.isnan(ce), np.isnan(ce2)) and np.allclose(ce, ce2, rtol=0, atol=0, equal_nan=True)
+
+
+def test_connected_components_two_components():
+    # components.zig:545-559: a U shape that merges late and a separate dot.
+    img = np.zeros((4, 6), np.uint8)
+    for x, y in [(0, 0), (0, 1), (0, 2), (1, 2), (2, 2), (2, 1), (2, 0), (5, 3)]:
+        img[y, x] = 255
+    n, lab, st, _ = O.connected_components(img, 8)
+    assert n == 3 and lab[0, 2] == 1 and lab[3, 5] == 2 and st[1, 4] == 7 and st[1, 2] == 3
+
+
+def test_adaptive_threshold_against_cv2():
+    # Mean: equal to cv2. Gaussian: equal but where the f32 blurred mean is
+    # within 1e-3 of a rounding tie (OpenCV 4 sums the f32 taps in another order).
+    import cv2
+    g = natural(240, 320, 1)
+    f = g.astype(np.float32)
+    for kind in (0, 1):
+        for block, delta in [(3, 0.0), (11, 2.5), (31, -3.2), (5, 7.0)]:
+            assert np.array_equal(O.adaptive_threshold(g, 255, 0, kind, block, delta),
+                                  cv2.adaptiveThreshold(g, 255, 0, kind, block, delta)), (kind, block, delta)
+            ours = O.adaptive_threshold(g, 200.4, 1, kind, block, delta)
+            ref = cv2.adaptiveThreshold(g, 200.4, 1, kind, block, delta)
+            bad = np.argwhere(ours != ref)
+            if len(bad):
+                m = O.gaussian_blur(f, (block, block), 0, 0, 1)
+                for y, x in bad:
+                    assert abs(abs(m[y, x] - np.floor(m[y, x])) - 0.5) < 1e-3, (kind, block, delta, y, x, m[y, x])
+
+
+def test_adaptive_threshold_refusals():
+    g = natural(20, 30, 1)
+    for args, want in [((255, 2, 0, 3, 0), -1), ((255, 0, 2, 3, 0), -1), ((255, 0, 0, 1, 0), -1), ((255, 0, 0, 4, 0), -1)]:
+        with pytest.raises(O.OracleError) as e:
+            O.adaptive_threshold(g, *args)
+        assert e.value.status == want, args
+    with pytest.raises(O.OracleError) as e:
+        O.adaptive_threshold(natural(20, 30, 3), 255, 0, 0, 3, 0)
+    assert e.value.status == -3
+
+
+def test_background_model_sequence():
+    rng = np.random.default_rng(5)
+    frames = [np.clip(natural(60, 80, 1).astype(int) + rng.integers(-40, 40, (60, 80)), 0, 255).astype(np.uint8)
+              for _ in range(6)]
+    for shift, t in [(4, 28), (0, 5), (15, 0)]:
+        bg = O.Background(80, 60, shift)
+        want = PT.background_ref(frames, shift, t)
+        for f, w_ in zip(frames, want):
+            assert np.array_equal(bg.apply(f, t), w_)
+        assert np.array_equal(bg.model, PT.background_model(frames, shift, t))

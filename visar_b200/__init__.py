@@ -56,6 +56,13 @@ def _load():
     lib.visar_undistort.argtypes = [ctypes.c_void_p, ctypes.c_void_p, dp, dp, ctypes.c_size_t, dp]
     lib.visar_init_undistort_rectify_map.argtypes = [dp, dp, ctypes.c_size_t, dp, dp, ctypes.c_void_p, ctypes.c_void_p]
     lib.visar_remap.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double]
+    lib.visar_connected_components.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int32),
+                                               ctypes.POINTER(ctypes.c_double), ctypes.c_size_t,
+                                               ctypes.POINTER(ctypes.c_size_t)]
+    lib.visar_background_create.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+    lib.visar_background_apply.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+    lib.visar_background_free.argtypes = [ctypes.c_void_p]
+    lib.visar_background_free.restype = None
     return lib
 
 
@@ -260,6 +267,62 @@ def remap(a, mapx, mapy, value=0.0, dst=None):
     _check(lib.visar_remap(ctypes.byref(desc(a)), ctypes.byref(desc(dst)), ctypes.byref(desc(mapx)),
                            ctypes.byref(desc(mapy)), ctypes.c_double(value)))
     return dst
+
+
+def equalize_hist(a, dst=None):
+    """visar_equalize_hist: 8U one channel."""
+    dst = _out(a, tuple(a.shape)) if dst is None else dst
+    _check(lib.visar_equalize_hist(ctypes.byref(desc(a)), ctypes.byref(desc(dst))))
+    return dst
+
+
+def adaptive_threshold(a, maxval, method, kind, block, delta, dst=None):
+    """visar_adaptive_threshold: method 0 MEAN_C / 1 GAUSSIAN_C, kind 0 BINARY / 1 BINARY_INV."""
+    dst = _out(a, tuple(a.shape)) if dst is None else dst
+    _check(lib.visar_adaptive_threshold(ctypes.byref(desc(a)), ctypes.byref(desc(dst)), ctypes.c_double(maxval),
+                                        int(method), int(kind), int(block), ctypes.c_double(delta)))
+    return dst
+
+
+def connected_components(a, connectivity=8, labels=None, max_stats=None):
+    """visar_connected_components: (count, labels int32, stats (n x 5 int32), centroids (n x 2 f64))."""
+    if labels is None:
+        if _is_torch(a):
+            import torch
+            labels = torch.empty(tuple(a.shape[:2]), dtype=torch.int32, device=a.device)
+        else:
+            labels = np.empty(tuple(a.shape[:2]), np.int32)
+    cap = max_stats if max_stats is not None else int(a.shape[0]) * int(a.shape[1]) + 1
+    stats = np.zeros((max(cap, 1), 5), np.int32)
+    cents = np.zeros((max(cap, 1), 2), np.float64)
+    n = ctypes.c_size_t(0)
+    _check(lib.visar_connected_components(ctypes.byref(desc(a)), ctypes.byref(desc(labels)), int(connectivity),
+                                          stats.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                          cents.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), cap, ctypes.byref(n)))
+    k = min(n.value, cap)
+    return n.value, labels, stats[:k], cents[:k]
+
+
+class Background:
+    """visar_background_*: the running-average background model (its state on the device)."""
+
+    def __init__(self, width, height, shift=4):
+        h = ctypes.c_void_p()
+        _check(lib.visar_background_create(ctypes.c_uint32(width), ctypes.c_uint32(height), int(shift), ctypes.byref(h)))
+        self._h = h
+
+    def apply(self, frame, threshold, mask=None):
+        mask = _out(frame, tuple(frame.shape)) if mask is None else mask
+        _check(lib.visar_background_apply(self._h, ctypes.byref(desc(frame)), ctypes.byref(desc(mask)), int(threshold)))
+        return mask
+
+    def close(self):
+        if getattr(self, "_h", None) and lib is not None:
+            lib.visar_background_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
 
 
 def gaussian_blur(a, ksize, sigma_x, sigma_y=0, border=4, dst=None):

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <stdexcept>
 #include <string>
@@ -1162,6 +1163,214 @@ int visar_remap(const visar_image *src, const visar_image *dst, const visar_imag
     ck(launch_remap(s.dev, d.dev, mx.dev, my.dev, bv, call.st));
     finish_out(call, d);
     end_call(call, s.host || d.host || mx.host || my.host);
+  });
+}
+
+}  // extern "C"
+
+// The background model's state: a u16 image on the device it was created on.
+struct visar_background {
+  int dev = 0;
+  uint32_t w = 0, h = 0;
+  int shift = 0;
+  bool primed = false;
+  uint16_t *model = nullptr;
+};
+
+extern "C" {
+
+// capi.zig:446-469 -> track.zig:17-82.
+int visar_background_create(uint32_t width, uint32_t height, int shift, visar_background **out) {
+  return guarded([&] {
+    if (!out) invalid_arg();
+    *out = nullptr;
+    if (shift < 0 || shift > 15) invalid_arg();
+    std::unique_ptr<visar_background> b(new visar_background);
+    ck(cudaGetDevice(&b->dev));
+    b->w = width;
+    b->h = height;
+    b->shift = shift;
+    if ((size_t)width * height > 0) ck(cudaMalloc(&b->model, (size_t)width * height * 2));
+    *out = b.release();
+  });
+}
+
+int visar_background_apply(visar_background *b, const visar_image *frame, const visar_image *mask, int threshold) {
+  return guarded([&] {
+    if (!b) invalid_arg();
+    std::lock_guard<std::mutex> lk(g_mu);
+    View f = typed(frame, k8U);
+    View m = typed(mask, k8U);
+    if (f.c->channels != 1 || f.c->width != m.c->width || f.c->height != m.c->height || f.c->channels != m.c->channels ||
+        f.c->width != b->w || f.c->height != b->h)
+      size_mismatch();
+    if (t_hint_dev >= 0 && t_hint_dev != b->dev) invalid_arg();
+    t_hint_dev = b->dev;
+    Call call = begin_call();
+    stage_in(call, f, kSrc);
+    stage_out(call, m, kDst);
+    ck(launch_background(f.dev, m.dev, b->model, std::min(std::max(threshold, 0), 255), b->shift, b->primed, call.st));
+    b->primed = true;
+    finish_out(call, m);
+    end_call(call, f.host || m.host);
+  });
+}
+
+void visar_background_free(visar_background *b) {
+  if (!b) return;
+  if (b->model) {
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(b->dev);
+    cudaFree(b->model);
+    cudaSetDevice(cur);
+  }
+  delete b;
+}
+
+// capi.zig:382-386 -> hist.zig:22-45.
+int visar_equalize_hist(const visar_image *src, const visar_image *dst) {
+  return guarded([&] {
+    std::lock_guard<std::mutex> lk(g_mu);
+    View s = typed(src, k8U);
+    View d = typed(dst, k8U);
+    if (s.c->channels != 1 || s.c->width != d.c->width || s.c->height != d.c->height || s.c->channels != d.c->channels)
+      size_mismatch();
+    Call call = begin_call();
+    stage_in(call, s, kSrc);
+    stage_out(call, d, kDst);
+    uint8_t *tab = static_cast<uint8_t *>(scratch(call, kSmall, 2048));
+    ck(launch_equalize_hist(s.dev, d.dev, reinterpret_cast<uint32_t *>(tab + 1024), tab, call.st));
+    finish_out(call, d);
+    end_call(call, s.host || d.host);
+  });
+}
+
+// capi.zig:326-337 -> threshold.zig:307-360: the mean (box, or the Gaussian of
+// an f32 copy rounded back to 8 bits; replicated border), then the compare.
+int visar_adaptive_threshold(const visar_image *src, const visar_image *dst, double maxval, int method, int type,
+                             int block, double delta) {
+  return guarded([&] {
+    if (method != 0 && method != 1) invalid_arg();
+    if (type != 0 && type != 1) invalid_arg();
+    if (block < 3) invalid_arg();
+    std::lock_guard<std::mutex> lk(g_mu);
+    View s = typed(src, k8U);
+    View d = typed(dst, k8U);
+    if (s.c->width != d.c->width || s.c->height != d.c->height || s.c->channels != d.c->channels) size_mismatch();
+    if (s.c->channels != 1) unsupported_channels();
+    if (block % 2 != 1) invalid_kernel();
+    // The filters' own kernel limits (boxFilter: 255, f32 gaussianBlur: 127).
+    if ((method == 0 && block > 255) || (method == 1 && block > 127)) invalid_kernel();
+    const int W = (int)s.c->width, H = (int)s.c->height;
+    Call call = begin_call();
+    stage_in(call, s, kSrc);
+    stage_out(call, d, kDst);
+    const size_t pitch = pitch_for(W);
+    DImg mean{static_cast<uint8_t *>(scratch(call, kTmp2, pitch * H)), (long long)pitch, W, H, 1};
+    SepSpec sp;
+    sp.border = kReplicate;
+    sp.shift = 0;
+    if (method == 0) {
+      sp.sdepth = sp.ddepth = k8U;
+      sp.scale = 1.0 / (double)(block * block);
+      sp.fin = kFinScaled;
+      sp.acc = kAccI32;
+      sp.kxi.assign(block, 1);
+      sp.kyi.assign(block, 1);
+      ck(launch_sep_filter(s.dev, mean, sp, call.st));
+    } else {
+      const size_t fp = pitch_for((long long)W * 4);
+      DImg f{static_cast<uint8_t *>(scratch(call, kTmp3, fp * H)), (long long)fp, W, H, 1};
+      DImg fb{static_cast<uint8_t *>(scratch(call, kTmp4, fp * H)), (long long)fp, W, H, 1};
+      ck(launch_convert_u8_f32(s.dev, f, true, call.st));
+      // gaussianBlur f32, sigma 0, kw = kh = block; a 1-pixel axis is not
+      // filtered (filter.zig:507-510).
+      const int kw = W == 1 ? 1 : block, kh = H == 1 ? 1 : block;
+      std::vector<double> kx(kw), ky(kh);
+      gaussian_kernel(kx.data(), kw, 0.0);
+      gaussian_kernel(ky.data(), kh, 0.0);
+      sp.sdepth = sp.ddepth = k32F;
+      sp.scale = 1.0;
+      sp.fin = kFinCast;
+      sp.acc = kAccF32;
+      for (double v : kx) sp.kxf.push_back((float)v);
+      for (double v : ky) sp.kyf.push_back((float)v);
+      ck(launch_sep_filter(f, fb, sp, call.st));
+      ck(launch_convert_u8_f32(fb, mean, false, call.st));
+    }
+    const double rv = std::nearbyint(maxval);
+    const uint8_t imax = (uint8_t)(rv != rv ? 0 : rv < 0 ? 0 : rv > 255 ? 255 : rv);
+    double dl = type == 0 ? std::ceil(delta) : std::floor(delta);
+    dl = dl != dl ? 0 : std::min(std::max(dl, -1024.0), 1024.0);
+    ck(launch_adaptive_cmp(s.dev, mean, d.dev, (int)dl, type == 1, imax, call.st));
+    finish_out(call, d);
+    end_call(call, s.host || d.host);
+  });
+}
+
+// capi.zig:529-551 -> components.zig:408-543.
+int visar_connected_components(const visar_image *src, const visar_image *labels, int connectivity, int32_t *stats,
+                               double *centroids, size_t max, size_t *count) {
+  return guarded([&] {
+    if (!count) invalid_arg();
+    std::lock_guard<std::mutex> lk(g_mu);
+    View s = typed(src, k8U);
+    View l = typed(labels, k32S);
+    if (s.c->channels != 1 || l.c->channels != 1 || s.c->width != l.c->width || s.c->height != l.c->height)
+      size_mismatch();
+    const long long W = s.c->width, H = s.c->height, n = W * H;
+    if (n >= (1LL << 31) - 1) fail(VISAR_INVALID_ARGUMENT, "InvalidSize");
+    const bool eight = connectivity != 4;
+    const long long nkeys = eight ? ((W + 1) / 2) * ((H + 1) / 2) : n;
+    Call call = begin_call();
+    stage_in(call, s, kSrc);
+    stage_out(call, l, kDst);
+    CcBuffers b;
+    b.P = static_cast<int *>(scratch(call, kTmp1, (size_t)n * 4));
+    b.K = static_cast<int *>(scratch(call, kTmp2, (size_t)n * 4));
+    b.F = static_cast<uint32_t *>(scratch(call, kTmp3, (size_t)nkeys * 4));
+    b.R = static_cast<uint32_t *>(scratch(call, kTmp4, (size_t)nkeys * 4));
+    b.tmp = static_cast<uint32_t *>(scratch(call, kTab1, cc_scan_tmp_words(nkeys) * 4));
+    uint32_t *small = static_cast<uint32_t *>(scratch(call, kSmall, 64));
+    b.err = reinterpret_cast<int *>(small);
+    b.total = small + 1;
+    ck(launch_cc_phase1(s.dev, eight, b, call.st));
+    uint32_t hs[2] = {0, 0};
+    ck(cudaMemcpyAsync(hs, small, 8, cudaMemcpyDeviceToHost, call.st));
+    ck(cudaStreamSynchronize(call.st));
+    if (hs[0]) fail(VISAR_INTERNAL, "Internal: union-find did not settle");
+    const int nl = (int)hs[1] + 1;
+    void *acc = scratch(call, kTab2, (size_t)nl * cc_acc_bytes());
+    ck(launch_cc_phase2(l.dev, eight, b, acc, nl, call.st));
+    const size_t want = std::min<size_t>(max, (size_t)nl);
+    std::vector<uint8_t> hacc(want * cc_acc_bytes());
+    if (want && (stats || centroids))
+      ck(cudaMemcpyAsync(hacc.data(), acc, hacc.size(), cudaMemcpyDeviceToHost, call.st));
+    finish_out(call, l);
+    ck(cudaGetLastError());
+    ck(cudaStreamSynchronize(call.st));
+    *count = (size_t)nl;
+    if (!stats && !centroids) return;
+    for (size_t i = 0; i < want; i++) {
+      long long a[7];
+      cc_read_acc(hacc.data(), (int)i, a);
+      const long long area = a[4];
+      if (stats) {
+        int32_t *o = stats + i * 5;
+        if (area == 0) {
+          o[0] = -1; o[1] = INT32_MAX; o[2] = 0; o[3] = 0; o[4] = 0;
+        } else {
+          o[0] = (int32_t)a[0]; o[1] = (int32_t)a[1]; o[2] = (int32_t)(a[2] - a[0] + 1); o[3] = (int32_t)(a[3] - a[1] + 1);
+          o[4] = (int32_t)area;
+        }
+      }
+      if (centroids) {
+        const double ar = (double)std::max<long long>(area, 1);
+        centroids[2 * i] = area == 0 ? NAN : (double)a[5] / 2.0 / ar;
+        centroids[2 * i + 1] = area == 0 ? NAN : (double)a[6] / ar;
+      }
+    }
   });
 }
 

@@ -546,6 +546,12 @@ struct MorphStrip {
   bool out_lane, live;
   Cols c;
   RowQueue q;
+  // kInside / kEdge: the next source row to fetch and the next output row,
+  // as running pointers at this lane's samples (advanced by a stride per
+  // row; rows outside [jlo, jhi) are fills and their pointers are not read).
+  const uint8_t *fp;
+  uint8_t *op;
+  int jlo, jhi, yout;
   uint32_t keep[4];     // kEdge: 16-bit lanes of samples inside the row
   uint32_t h1[KH1][4];  // the first pass's input rows
   uint32_t h2[KH2][4];  // the second pass's input rows (first-pass results)
@@ -563,37 +569,46 @@ struct MorphStrip {
     out_lane = lane >= HALO && lane < 32 - HALO && gs < n;
     live = gs < n && gs + kSPL > 0;
     q = row_queue(lane);
+    jlo = max(0, -first);
+    jhi = max(jlo, min(nsrc, H - first));
+    if (!live) jhi = jlo;  // kEdge: lanes without samples in the row only fill
+    fp = s.p + (long long)first * s.stride + gs;
+    yout = y0;
+    op = d.p + (long long)y0 * d.stride + gs;
   }
 
-  // Source row j into its slot (rows j >= nsrc: nothing is read).
+  // Source row j into its slot (rows j >= nsrc: nothing is read). kInside and
+  // kEdge fetch rows in order, one per call.
   template <int MODE>
   __device__ __forceinline__ void fetch(int j) {
-    const int sy = first + j;
-    const bool in = sy >= 0 && sy < H;
-    if constexpr (MODE == kInside) {
-      fetch8_inside(q.slot(j), row_ptr<const uint8_t>(s, in ? sy : 0) + gs, in && j < nsrc, I1);
-    } else if constexpr (MODE == kEdge) {
-      fetch8_inside(q.slot(j), row_ptr<const uint8_t>(s, in ? sy : 0) + gs, in && j < nsrc && live, I1);
+    if constexpr (MODE != kSlow) {
+      fetch8_inside(q.slot(j), fp, (unsigned)(j - jlo) < (unsigned)(jhi - jlo), I1);
+      fp += s.stride;
     } else {
+      const int sy = first + j;
+      const bool in = sy >= 0 && sy < H;
       if (j < nsrc) fetch8(q.slot(j), in ? row_ptr<const uint8_t>(s, sy) : nullptr, c, I1);
     }
   }
 
-  // Output row y, written when it belongs to the tile and the image.
+  // Output row y, written when it belongs to the tile and the image. kInside
+  // and kEdge put rows y0, y0 + 1, ... in order, one per call.
   template <int MODE>
   __device__ __forceinline__ void put(int y, const uint32_t (&o)[4]) {
     const uint2 o8 = pack_pairs(o);
-    const bool ok = out_lane && y < ylim;
     if constexpr (MODE != kSlow) {
-      st_global8_if(row_ptr<uint8_t>(d, ok ? y : 0) + gs, o8, ok);
+      st_global8_if(op, o8, out_lane && yout < ylim);
+      op += d.stride;
+      yout++;
     } else {
-      if (ok) store8(row_ptr<uint8_t>(d, y), gs, n, o8.x, o8.y);
+      if (out_lane && y < ylim) store8(row_ptr<uint8_t>(d, y), gs, n, o8.x, o8.y);
     }
   }
 
   // Source row j; PH = j mod KH1. Rows past nsrc (the last group of KH1)
-  // compute values that are not stored.
-  template <int MODE, int PH>
+  // compute values that are not stored. WARM: j may still be inside the
+  // first rows that only fill the windows (checked per row, uniform).
+  template <int MODE, bool WARM, int PH>
   __device__ __forceinline__ void step(int j) {
     cp_wait<kQD - 1>();  // row j has landed
     const uint2 cur = ld_shared8(q.slot(j));
@@ -604,7 +619,7 @@ struct MorphStrip {
 #pragma unroll
       for (int p = 0; p < 4; p++) h1[PH][p] = (h1[PH][p] & keep[p]) | (I1p & ~keep[p]);
     }
-    if (j < KH1 - 1) return;
+    if (WARM && j < KH1 - 1) return;
     uint32_t o1[4];
     band_apply<P1, CN, MAX1, (PH + 1) % KH1>(h1, o1);
     const int y1 = first + j - (KH1 - 1) + AY1;  // first-pass row completed
@@ -621,16 +636,16 @@ struct MorphStrip {
         h2[S2][p] = MODE == kEdge ? (v & keep[p]) | (I2p & ~keep[p]) : v;
       }
       if constexpr (MODE == kSlow) mask_pairs(h2[S2], c, I2p);
-      if (j < (KH1 - 1) + (KH2 - 1)) return;
+      if (WARM && j < (KH1 - 1) + (KH2 - 1)) return;
       uint32_t o2[4];
       band_apply<P2, CN, MAX2, (PH + 2) % KH2>(h2, o2);
       put<MODE>(y1 - (KH2 - 1) + AY2, o2);
     }
   }
 
-  template <int MODE, int... PH>
+  template <int MODE, bool WARM, int... PH>
   __device__ __forceinline__ void steps(int j, std::integer_sequence<int, PH...>) {
-    (step<MODE, PH>(j + PH), ...);
+    (step<MODE, WARM, PH>(j + PH), ...);
   }
 
   template <int MODE>
@@ -648,7 +663,7 @@ struct MorphStrip {
       cp_commit();
     }
 #pragma unroll 1
-    for (int j = 0; j < nsrc; j += KH1) steps<MODE>(j, std::make_integer_sequence<int, KH1>{});
+    for (int j = 0; j < nsrc; j += KH1) steps<MODE, true>(j, std::make_integer_sequence<int, KH1>{});
   }
 
   // pad: bit 0 = source rows readable, bit 1 = destination rows writable, up

@@ -11,9 +11,9 @@
 
 namespace vb {
 
-enum Depth : int { k8U = 0, k16U = 2, k16S = 3, k32F = 5 };
+enum Depth : int { k8U = 0, k16U = 2, k16S = 3, k32S = 4, k32F = 5 };
 
-inline int depth_size(int d) { return d == k8U ? 1 : (d == k16U || d == k16S) ? 2 : d == k32F ? 4 : 0; }
+inline int depth_size(int d) { return d == k8U ? 1 : (d == k16U || d == k16S) ? 2 : (d == k32F || d == k32S) ? 4 : 0; }
 
 // Counts kernel launches made by the library (reported by visar_cuda_launch_count).
 void note_launch(int n = 1);
@@ -131,6 +131,29 @@ bool undistort_map_params(const double K[9], const double k8[8], const double *R
 cudaError_t launch_undistort(const DImg &s, const DImg &d, const void *stripes_dev, cudaStream_t st);
 cudaError_t launch_init_undistort_map(const std::vector<uint8_t> &params, const DImg &mx, const DImg &my, cudaStream_t st);
 cudaError_t launch_remap(const DImg &s, const DImg &d, const DImg &mx, const DImg &my, uint8_t value, cudaStream_t st);
+
+// ------------------------------------------- tracker tail (tail.cu)
+cudaError_t launch_equalize_hist(const DImg &s, const DImg &d, uint32_t *hist_dev, uint8_t *lut_dev, cudaStream_t st);
+cudaError_t launch_adaptive_cmp(const DImg &s, const DImg &m, const DImg &d, int idelta, bool inv, uint8_t imax,
+                                cudaStream_t st);
+cudaError_t launch_convert_u8_f32(const DImg &s, const DImg &d, bool to_f32, cudaStream_t st);
+cudaError_t launch_background(const DImg &f, const DImg &m, uint16_t *model, int t, int shift, bool primed, cudaStream_t st);
+// Connected components: device work buffers (P, K: one int per pixel; F, R:
+// one u32 per key; tmp: cc_scan_tmp_words(keys) u32; err, total: one each).
+struct CcBuffers {
+  int *P, *K;
+  uint32_t *F, *R, *tmp;
+  int *err;
+  uint32_t *total;
+};
+size_t cc_scan_tmp_words(long long n);
+size_t cc_acc_bytes();
+// Labels by union-find, keys, ranks; *total receives the component count.
+cudaError_t launch_cc_phase1(const DImg &s, bool eight, const CcBuffers &b, cudaStream_t st);
+// The label image and per-label accumulators (nlabels = components + 1).
+cudaError_t launch_cc_phase2(const DImg &labels, bool eight, const CcBuffers &b, void *acc, int nlabels, cudaStream_t st);
+// x0, y0, x1, y1, area, twice the x sum, y sum of accumulator i (host copy).
+void cc_read_acc(const void *host_acc, int i, long long out[7]);
 
 // ------------------------------------------------------- host helpers
 // Gaussian taps (src/imgproc/filter.zig:350-476), in host f64.
