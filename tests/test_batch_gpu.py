@@ -182,6 +182,32 @@ def test_thresholds_warps_and_borders():
                       ("resize", {"fx": 0.5, "fy": 0.5, "interp": 3})])
 
 
+def test_gauss_strip_every_border_and_edge_geometry():
+    """The binomial 3x3 / 5x5 strips under every border (wrap through the
+    general kernel), on images whose rows end at every offset within a lane
+    and a strip, down to 1-3 rows and columns, in 1, 3 and 4 channels, with
+    every tile height."""
+    rng = np.random.default_rng(71)
+    shapes = [(1, 1), (2, 3), (3, 2), (3, 17), (5, 5), (9, 1), (1, 40)]
+    shapes += [(int(rng.integers(4, 140)), int(w)) for w in list(range(236, 252)) + list(range(1, 20, 3))]
+    shapes += [(300, 481), (257, 719), (64, 240), (65, 241)]
+    imgs = [synth.base_image_torch(h, w, [1, 3, 4][k % 3], nrect=3, seed=700 + k) for k, (h, w) in enumerate(shapes)]
+    try:
+        for rows in (8, 32, 64):
+            B.tune_load(None)
+            for cn in (1, 3, 4):
+                for k in (3, 5):
+                    B.tune_set(f"gauss_strip.u8.c{cn}.k{k}.rows", rows)
+            for k in (3, 5):
+                for border in range(5):
+                    plan = check_plan(imgs, [("gauss", {"k": (k, k), "border": border})])
+                    # Wrap takes the general kernel (its border columns come from the row's far end).
+                    assert any(st["name"].startswith("gauss_strip") for st in plan.launch_stats()) == (border != 3)
+                    del plan
+    finally:
+        B.tune_load(None)
+
+
 def test_every_strip_profile_fused_and_single():
     """Each compiled element profile (rect 3/5/7, cross 3/5, ellipse 5/7) as
     erode, dilate and the fused open / close, on 1-, 3- and 4-channel images."""

@@ -433,10 +433,16 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
         if (u8) {
           std::vector<int64_t> t(kw);
           gaussian_kernel_fixed(t.data(), kw, sx, 8);
-          if (binomial_taps(t) && u8_aligned8(im.v)) {
+          // Strips map rows past the bottom edge in closed form (images taller
+          // than the radius) and take border columns from their own row
+          // window (not the far end of the row: no wrap); they write whole
+          // 8-byte words into padded destination rows.
+          if (binomial_taps(t) && u8_aligned8(im.v) && im.v.h > kw / 2 && border != kWrap && next[i].padded) {
             Launch *l = class_of(ls, kOpGaussStrip, k8U, im.v.cn, kw, false);
             l->border = border;
-            add_img(l, bimg(im.v, next[i].v), im.input);
+            BImg b = bimg(im.v, next[i].v);
+            b.pad = (im.padded && im.input < 0 ? 1 : 0) | 2;
+            add_img(l, b, im.input);
             u8_bytes(*l, im.v, next[i].v, 1);
             continue;
           }

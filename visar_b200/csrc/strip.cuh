@@ -233,74 +233,223 @@ __device__ __forceinline__ void st_global8_if(uint8_t *g, uint2 v, bool p) {
 // rows [ty*RH, ty*RH + RH). The vertical binomial runs as a cascade of
 // pairwise sums over the incoming rows (its state alternates between two
 // register sets, ca and cb, so consecutive rows need no moves); the
-// horizontal one on the pairs of this lane and its neighbours.
+// horizontal one on the pairs of this lane and its neighbours, scaled so that
+// the result is each 16-bit lane's high byte: (F*H + 2^7) >> 8 with
+// F = 2^(8-SH) equals (H + 2^(SH-1)) >> SH.
+//
+// Lanes that start inside the row copy 8 bytes of it into their slot of the
+// row queue (the source rows are readable up to their length rounded up to 8
+// samples, except the last row of an unpadded image, whose end is read
+// bytewise) and the others fill theirs; each lane then takes its samples
+// from a 16-byte window of the warp's slot, byte k from window byte u_k,
+// three byte permutes per 4-byte word (in a row's inner strips the window
+// holds the lane's own bytes, unpermuted). Samples outside
+// the row within the stencil's reach are thereby border-mapped (the sample of
+// the mapped pixel, same channel; the window always covers them for the
+// constant, replicate, reflect and reflect-101 borders), and constant-border
+// ones are masked to zero. A slot is refilled only after every lane has read
+// it: row j + kGQ - 1 goes into row j - 1's slot once a warp barrier has
+// seen every lane past row j - 1 (so kGQ - 1 rows are in flight). Every
+// tile takes this one path: a separate one for inner strips doubles the
+// loop's code and its registers. The selectors live in shared memory and are
+// read per row, which keeps them out of the loop's registers.
+constexpr int kGQ = 16;  // row queue depth of the Gaussian strips
+
+struct GaussQueue {
+  uint32_t base;  // shared address of this lane's bytes in slot 0
+  uint32_t par;   // shared address of this lane's window selectors
+  __device__ __forceinline__ uint32_t slot(int j) const { return base + (uint32_t)((j & (kGQ - 1)) * 32 * kSPL); }
+};
+
+__device__ __forceinline__ GaussQueue gauss_queue(int lane) {
+  __shared__ __align__(16) uint2 s_gq[kWarpsPerBlock][kGQ][32];
+  __shared__ __align__(16) uint4 s_gp[kWarpsPerBlock][32][2];
+  const int w = (threadIdx.x >> 5) % kWarpsPerBlock;
+  return GaussQueue{(uint32_t)__cvta_generic_to_shared(&s_gq[w][0][lane]),
+                    (uint32_t)__cvta_generic_to_shared(&s_gp[w][lane][0])};
+}
+
+__device__ __forceinline__ uint4 ld_shared16(uint32_t saddr) {
+  uint4 v;
+  asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];\n" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "r"(saddr));
+  return v;
+}
+__device__ __forceinline__ void st_shared16(uint32_t saddr, uint4 v) {
+  asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};\n" ::"r"(saddr), "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w));
+}
+
 template <int K, int CN, int RH>
 struct GaussStrip {
   using G = GaussGeom<K, CN>;
   static constexpr int R = G::R, HALO = G::HALO;
-  static constexpr int NR = RH + K - 1;
   static constexpr int E = Binom<K>::e;
   static constexpr int SH = 16 - 2 * E;
-  static constexpr uint32_t RND = (1u << (SH - 1)) * 0x00010001u;
+  static_assert(SH <= 8, "the scaled sum must fit a 16-bit lane");
+  static constexpr uint32_t F = 1u << (8 - SH);
+  static constexpr uint32_t RND = 0x00800080u;
+  static constexpr int QD = kGQ - 1;  // rows in flight
 
   const DImg s, d;  // copies (kept in registers across the row loop)
-  int border, y0, nr;
+  int border, pad, H, first, nr, ylim, yout;
   long long n, gs;
-  bool out_lane;
-  Cols c;
-  RowQueue q;
-  int lo[R], hi[R];  // border-mapped rows -R..-1 and h..h+R-1 (-1: constant fill)
+  bool out_lane, from;
+  GaussQueue q;
+  // The next source row to fetch and the next output row, at this lane's
+  // samples (advanced by a stride per row).
+  const uint8_t *fp;
+  uint8_t *op;
   uint32_t ca[K - 1][4], cb[K - 1][4];
+  int woff;  // window offset from this lane's slot
 
-  __device__ __forceinline__ GaussStrip(const DImg &s_, const DImg &d_, int border_, int tx, int ty, int lane)
-      : s(s_), d(d_), border(border_), y0(ty * RH) {
+  __device__ __forceinline__ GaussStrip(const DImg &s_, const DImg &d_, int border_, int pad_, int tx, int ty,
+                                        int lane)
+      : s(s_), d(d_), border(border_), pad(pad_) {
     n = (long long)s.w * CN;
     gs = ((long long)tx * G::OL - HALO + lane) * kSPL;
-    c = make_cols<CN, G::REACH>(gs, n, s.w, border, false, lane);
     out_lane = lane >= HALO && lane < 32 - HALO && gs < n;
-    q = row_queue(lane);
+    from = gs >= 0 && gs < n;
+    q = gauss_queue(lane);
+    H = s.h;
+    const int y0 = ty * RH;
+    first = y0 - R;
     // Only the rows the tile's outputs (y < h) need: at most R past the image.
-    nr = min(NR, d.h - y0 + K - 1);
-#pragma unroll
-    for (int r = 0; r < R; r++) {
-      lo[r] = border_map(r - R, s.h, border);
-      hi[r] = border_map(s.h + r, s.h, border);
-    }
+    ylim = min(y0 + RH, d.h);
+    nr = min(RH + K - 1, ylim - y0 + K - 1);
+    fp = s.p + (long long)first * s.stride + gs;
+    op = d.p + (long long)y0 * d.stride + gs;
+    yout = y0;
   }
 
-  // Image row of source row j (y0 - R + j, border-mapped; -1: constant fill).
-  __device__ __forceinline__ int map_row(int j) const {
-    const int sy = y0 - R + j;
-    int my = sy;
-#pragma unroll
-    for (int r = 0; r < R; r++) {
-      my = sy == r - R ? lo[r] : my;
-      my = sy == s.h + r ? hi[r] : my;
+  // The window and selectors of this lane (see above), stored at q.par:
+  // {a0, b0, m0, a1}, {b1, m1, keep0, keep1} for the first-level permutes of
+  // window bytes 0-7 (a) and 8-15 (b), the merge (m) and the
+  // constant-border masks of words 0 and 1.
+  // Where byte k of this lane comes from: 0 = not needed (outside the
+  // stencil's reach), 1 = strip byte t, 2 = zero (constant border).
+  __device__ __forceinline__ int byte_src(int k, long long base, long long need_lo, long long need_hi, int &t) const {
+    const long long g = gs + k;
+    if (g < need_lo || g >= need_hi) return 0;
+    if (g >= 0 && g < n) {
+      t = (int)(g - base);
+      return 1;
     }
-    return my;
+    const long long px = g >= 0 ? g / CN : -((-g + CN - 1) / CN);
+    const int mx = border_map(px, s.w, border);
+    if (mx < 0) return 2;
+    t = (int)((long long)mx * CN + (g - px * CN) - base);
+    return 1;
   }
 
-  // Source row j into its slot (rows j >= nr: nothing is read).
-  template <bool INSIDE>
+  __device__ __forceinline__ void edge_setup(int lane) {
+    const long long base = gs - (long long)lane * kSPL;  // the strip's first sample
+    const long long need_lo = base + kSPL * HALO - G::REACH;
+    const long long need_hi = min(base + kSPL * (32 - HALO), n) + G::REACH;
+    int lo = 1 << 30;
+    unsigned long long keep = ~0ull;
+#pragma unroll 1
+    for (int k = 0; k < kSPL; k++) {
+      int t = 0;
+      const int r = byte_src(k, base, need_lo, need_hi, t);
+      if (r == 1) lo = min(lo, t);
+      if (r == 2) keep &= ~(0xFFull << (8 * k));
+    }
+    const int W = min(lo == (1 << 30) ? lane * kSPL : lo & ~7, 256 - 16);
+    woff = W - lane * kSPL;
+    uint32_t sa[2] = {0, 0}, sb[2] = {0, 0}, sm[2] = {0, 0};
+#pragma unroll 1
+    for (int k = 0; k < kSPL; k++) {
+      int t = W;
+      const int r = byte_src(k, base, need_lo, need_hi, t);
+      const int u = r == 1 ? (t - W) & 15 : 0;
+      const int sh = 4 * (k & 3);
+      const uint32_t a = u < 8 ? (uint32_t)u << sh : 0u, b = u < 8 ? 0u : (uint32_t)(u - 8) << sh;
+      const uint32_t m = (uint32_t)((u < 8 ? 0 : 4) + (k & 3)) << sh;
+      if (k < 4) {
+        sa[0] |= a, sb[0] |= b, sm[0] |= m;
+      } else {
+        sa[1] |= a, sb[1] |= b, sm[1] |= m;
+      }
+    }
+    st_shared16(q.par, make_uint4(sa[0], sb[0], sm[0], sa[1]));
+    st_shared16(q.par + 16, make_uint4(sb[1], sm[1], (uint32_t)keep, (uint32_t)(keep >> 32)));
+  }
+
+  // The row end of the last row of an unpadded image (cnt < 8 bytes), bytewise.
+  static __device__ __forceinline__ uint2 load_row_end(const uint8_t *p, int cnt) {
+    uint32_t v[2] = {0, 0};
+#pragma unroll
+    for (int k = 0; k < kSPL; k++)
+      if (k < cnt) v[k >> 2] |= (uint32_t)__ldg(p + k) << (8 * (k & 3));
+    return make_uint2(v[0], v[1]);
+  }
+
+  // Source row j into its slot (rows j >= nr: nothing is read). Rows are
+  // fetched in order, one per call; rows past the top or bottom edge (a
+  // warp-uniform case) are border-mapped, -1 being the constant fill. PRO:
+  // the first rows of the queue, which hold every row above the image
+  // (R < kQD - 1); the later ones can only pass the bottom, by less than R
+  // rows where it matters (j < nr), which the map below covers for images
+  // taller than R.
+  template <bool PRO>
   __device__ __forceinline__ void fetch(int j) {
-    const int my = map_row(j);
-    if constexpr (INSIDE) {
-      const uint8_t *row = row_ptr<const uint8_t>(s, my < 0 ? 0 : my);
-      fetch8_inside(q.slot(j), row + gs, my >= 0 && j < nr, 0u);
+    const int sy = first + j;
+    const uint8_t *p = fp;
+    fp += s.stride;
+    bool ok = j < nr;
+    int my = sy;
+    if constexpr (PRO) {
+      if ((unsigned)sy >= (unsigned)H) {
+        my = border_map(sy, H, border);
+        ok = ok && my >= 0;
+        p += (long long)(my - sy) * s.stride;
+      }
     } else {
-      if (j < nr) fetch8(q.slot(j), my < 0 ? nullptr : row_ptr<const uint8_t>(s, my), c, 0u);
+      if (sy >= H) {
+        my = border == kReplicate    ? H - 1
+             : border == kReflect    ? 2 * H - 1 - sy
+             : border == kReflect101 ? 2 * H - 2 - sy
+             : border == kWrap       ? sy - H
+                                     : -1;
+        ok = ok && (unsigned)my < (unsigned)H;
+        p += (long long)(my - sy) * s.stride;
+      }
     }
+    // Lanes starting inside the row copy 8 bytes; a lane straddling the end
+    // of an unpadded image's last row reads the row end bytewise.
+    if (!(pad & 1) && my == H - 1 && from && gs + kSPL > n)
+      st_shared8(q.slot(j), ok ? load_row_end(p, (int)(n - gs)) : make_uint2(0, 0));
+    else
+      fetch8_inside(q.slot(j), p, ok && from, 0u);
   }
 
-  // Source row j. OUT: the cascade is full (j >= K - 1) and row j - (K - 1)
-  // is written when it lies in the image.
-  template <bool INSIDE, bool ODD, bool OUT>
+  // This lane's 8 samples of row j from its window of the slot.
+  __device__ __forceinline__ uint2 window(int j) const {
+    const uint32_t a = q.slot(j) + woff;
+    const uint4 p0 = ld_shared16(q.par), p1 = ld_shared16(q.par + 16);
+    const uint2 w0 = ld_shared8(a), w1 = ld_shared8(a + 8);
+    const uint32_t x0 = __byte_perm(__byte_perm(w0.x, w0.y, p0.x), __byte_perm(w1.x, w1.y, p0.y), p0.z);
+    const uint32_t x1 = __byte_perm(__byte_perm(w0.x, w0.y, p0.w), __byte_perm(w1.x, w1.y, p1.x), p1.y);
+    return make_uint2(x0 & p1.z, x1 & p1.w);
+  }
+
+  // The next output row (rows past the tile or the image are not written;
+  // lanes write 8 bytes, into the destination's row padding at the end).
+  __device__ __forceinline__ void put(const uint32_t (&h)[4]) {
+    const uint2 o8 = make_uint2(__byte_perm(h[0], h[1], 0x7531), __byte_perm(h[2], h[3], 0x7531));
+    st_global8_if(op, o8, out_lane && yout < ylim);
+    op += d.stride;
+    yout++;
+  }
+
+  // Source row j; the output row j - (K - 1) once the cascade is full.
+  template <bool ODD>
   __device__ __forceinline__ void step(int j) {
     const uint32_t(&in)[K - 1][4] = ODD ? cb : ca;
     uint32_t(&out)[K - 1][4] = ODD ? ca : cb;
-    cp_wait<kQD - 1>();  // row j has landed
-    const uint2 cur = ld_shared8(q.slot(j));
-    fetch<INSIDE>(j + kQD);
+    cp_wait<QD - 1>();  // row j has landed
+    __syncwarp();  // every lane's row j has landed; every read of row j - 1's slot is done
+    fetch<false>(j + QD);
+    const uint2 cur = window(j);
     cp_commit();
     // Cascade of pairwise sums: after row j the last stage holds the
     // binomial sum of rows j-K+1..j.
@@ -314,69 +463,56 @@ struct GaussStrip {
         out[a][i] = v[i];
         v[i] = t;
       }
-    if constexpr (!OUT) return;
+    if (j < K - 1) return;
     Window<HALO, -G::REACH, kSPL - 1 + G::REACH> win;
     win.gather(v);
     uint32_t h[4];
 #pragma unroll
     for (int o = 0; o < 4; o++) {
       const int c0 = 2 * o;
+      const uint32_t x = win.at(c0);
+      uint32_t sum;
       if constexpr (K == 3) {
-        h[o] = win.at(c0 - CN) + win.at(c0 + CN) + (win.at(c0) << 1) + RND;
+        sum = win.at(c0 - CN) + win.at(c0 + CN) + (x << 1);
       } else {
-        // a + 4 b + 6 x = (l2 + r2) + 4 (l1 + r1 + x) + 2 x
-        const uint32_t x = win.at(c0);
-        const uint32_t a = win.at(c0 - 2 * CN) + win.at(c0 + 2 * CN) + RND;
-        const uint32_t b = win.at(c0 - CN) + win.at(c0 + CN) + x;
-        h[o] = a + (b << 2) + (x << 1);
+        // a + 4 b + 6 x
+        const uint32_t a = win.at(c0 - 2 * CN) + win.at(c0 + 2 * CN);
+        const uint32_t b = win.at(c0 - CN) + win.at(c0 + CN);
+        sum = a + (b << 2) + x * 6u;
       }
-      h[o] >>= SH;
+      h[o] = sum * F + RND;
     }
-    const int y = y0 + j - (K - 1);
-    const bool ok = out_lane && y < d.h;
-    const uint2 o8 = pack_pairs(h);
-    if constexpr (INSIDE) {
-      st_global8_if(row_ptr<uint8_t>(d, ok ? y : 0) + gs, o8, ok);
-    } else {
-      if (ok) store8(row_ptr<uint8_t>(d, y), gs, n, o8.x, o8.y);
-    }
+    put(h);
   }
 
-  template <bool INSIDE>
-  __device__ __forceinline__ void rows() {
-    static_assert((K - 1) % 2 == 0, "the cascade fills in pairs of rows");
+  __device__ __forceinline__ void rows(int lane) {
+    edge_setup(lane);
 #pragma unroll 1
-    for (int j = 0; j < kQD; j++) {
-      fetch<INSIDE>(j);
+    for (int j = 0; j < QD; j++) {
+      fetch<true>(j);
       cp_commit();
     }
 #pragma unroll
     for (int a = 0; a < K - 1; a++)
 #pragma unroll
       for (int i = 0; i < 4; i++) ca[a][i] = 0;
+    // Pairs of rows; rows past nr are neither read nor stored.
 #pragma unroll 1
-    for (int j = 0; j < K - 1; j += 2) {
-      step<INSIDE, false, false>(j);
-      step<INSIDE, true, false>(j + 1);
+    for (int j = 0; j < nr; j += 2) {
+      step<false>(j);
+      step<true>(j + 1);
     }
-    // Pairs of rows; an odd nr ends with one row past the image (not stored).
-#pragma unroll 1
-    for (int j = K - 1; j < nr; j += 2) {
-      step<INSIDE, false, true>(j);
-      step<INSIDE, true, true>(j + 1);
-    }
-  }
-
-  __device__ __forceinline__ void run() {
-    if (__all_sync(kFull, c.inside)) rows<true>();
-    else rows<false>();
   }
 };
 
+// pad: bit 0 = source rows readable up to their length rounded up to 8
+// samples (all but the last row always are: strips take 8-byte aligned rows),
+// bit 1 = the same for destination rows, which the strip requires.
 template <int K, int CN, int RH>
-__device__ __forceinline__ void gauss_strip(const DImg &s, const DImg &d, int border, int tx, int ty, int lane) {
-  GaussStrip<K, CN, RH> g(s, d, border, tx, ty, lane);
-  g.run();
+__device__ __forceinline__ void gauss_strip(const DImg &s, const DImg &d, int border, int pad, int tx, int ty,
+                                            int lane) {
+  GaussStrip<K, CN, RH> g(s, d, border, pad, tx, ty, lane);
+  g.rows(lane);
 }
 
 // ---------------------------------------------------------- morphology
