@@ -7,6 +7,7 @@ operation order; host code gets -ffp-contract=off for the same reason.
 Usage: python visar_b200/build.py [--force]   (the package import needs the built library)
 """
 import os
+import re
 import subprocess
 import sys
 from concurrent.futures import ThreadPoolExecutor
@@ -30,18 +31,29 @@ def _sources():
     return out
 
 
-def _headers_mtime():
-    m = 0.0
-    for d in (CSRC, os.path.join(HERE, "..", "include")):
-        for f in os.listdir(d):
-            if f.endswith((".h", ".cuh", ".hpp")):
-                m = max(m, os.path.getmtime(os.path.join(d, f)))
+_INCLUDE = re.compile(r'^\s*#\s*include\s+"([^"]+)"', re.M)
+
+
+def _deps_mtime(src, seen=None):
+    """Newest modification time of src and the local headers it includes (recursively)."""
+    seen = set() if seen is None else seen
+    m = os.path.getmtime(src)
+    with open(src, errors="replace") as f:
+        text = f.read()
+    for name in _INCLUDE.findall(text):
+        for d in (os.path.dirname(src), CSRC, os.path.join(HERE, "..", "include")):
+            path = os.path.normpath(os.path.join(d, name))
+            if os.path.exists(path):
+                if path not in seen:
+                    seen.add(path)
+                    m = max(m, _deps_mtime(path, seen))
+                break
     return m
 
 
-def _compile(src, force, hdr_m):
+def _compile(src, force):
     obj = os.path.join(OBJ, os.path.basename(src) + ".o")
-    if not force and os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(src), hdr_m):
+    if not force and os.path.exists(obj) and os.path.getmtime(obj) >= _deps_mtime(src):
         return obj, None
     if src.endswith(".cu"):
         cmd = [NVCC] + NVCC_FLAGS + ["-c", src, "-o", obj]
@@ -57,9 +69,10 @@ def build(force=False, verbose=False):
     """Compiles every source under csrc/ and links libvisar_b200.so; returns its path."""
     os.makedirs(OBJ, exist_ok=True)
     srcs = _sources()
-    hdr_m = _headers_mtime()
+    # The slowest units first, so that they do not start last.
+    srcs.sort(key=lambda f: -os.path.getsize(f) if "strip" not in f else -1e9)
     with ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 4)) as ex:
-        results = list(ex.map(lambda s: _compile(s, force, hdr_m), srcs))
+        results = list(ex.map(lambda s: _compile(s, force), srcs))
     errs = [e for _, e in results if e]
     if errs:
         raise RuntimeError("visar_b200 build failed:\n" + "\n".join(errs))

@@ -848,6 +848,19 @@ cudaError_t launch_morph_strip_prof(const LaunchRun &r, int rows, bool max1, boo
   return launch_morph_strip_rh<PR, CN, 32>(r, max1, fused, st);
 }
 
+// The one-channel profiles are instantiated in units of their own
+// (batch_strip1a/b/c.cu).
+#define VB_MORPH_PROF1(P) \
+  extern template cudaError_t launch_morph_strip_prof<strip::P, 1>(const LaunchRun &, int, bool, bool, cudaStream_t);
+VB_MORPH_PROF1(ProfRect3)
+VB_MORPH_PROF1(ProfRect5)
+VB_MORPH_PROF1(ProfRect7)
+VB_MORPH_PROF1(ProfCross3)
+VB_MORPH_PROF1(ProfCross5)
+VB_MORPH_PROF1(ProfEll5)
+VB_MORPH_PROF1(ProfEll7)
+#undef VB_MORPH_PROF1
+
 template <int CN>
 cudaError_t launch_morph_strip_cn(const LaunchRun &r, int prof, int rows, bool max1, bool fused, cudaStream_t st) {
   using namespace strip;

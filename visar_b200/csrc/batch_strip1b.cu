@@ -1,0 +1,13 @@
+// Morphology strip launches of the batched form for one-channel images:
+// elements Rect7, Cross3, Cross5.
+#include "batch.cuh"
+
+namespace vb {
+namespace bt {
+
+template cudaError_t launch_morph_strip_prof<strip::ProfRect7, 1>(const LaunchRun &, int, bool, bool, cudaStream_t);
+template cudaError_t launch_morph_strip_prof<strip::ProfCross3, 1>(const LaunchRun &, int, bool, bool, cudaStream_t);
+template cudaError_t launch_morph_strip_prof<strip::ProfCross5, 1>(const LaunchRun &, int, bool, bool, cudaStream_t);
+
+}  // namespace bt
+}  // namespace vb
