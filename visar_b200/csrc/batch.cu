@@ -764,6 +764,8 @@ cudaError_t run_morph(const Plan &P, const Launch &L, cudaStream_t st) {
 
 template <class T, bool PERSP>
 cudaError_t run_warp(const Plan &P, const Launch &L, cudaStream_t st) {
+  // Pool destinations are pitched (4-byte aligned rows).
+  if (sizeof(T) == 1 && L.cn == 1 && L.wa.interp != 0) return run_op<OpWarp4<PERSP>>(P, L, L.wa, st);
   switch (L.cn) {
     case 1: return run_op<OpWarp<T, 1, PERSP>>(P, L, L.wa, st);
     case 3: return run_op<OpWarp<T, 3, PERSP>>(P, L, L.wa, st);

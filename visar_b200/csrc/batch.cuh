@@ -777,6 +777,40 @@ struct OpWarp {
   }
 };
 
+// One-channel u8 warpAffine / warpPerspective, INTER_LINEAR, on 32 x 32
+// output tiles of four consecutive pixels per thread (wp::warp4_u8: the
+// taps of four pixels in flight together, 4-byte stores); a warp covers
+// 32 x 4 pixels.
+template <bool PERSP>
+struct OpWarp4 {
+  static constexpr int kThreads = 256, TS = 32, kMinBlocks = 3;  // <= 85 registers (no spills)
+  using Args = WarpArgs;
+  static size_t smem(const Args &) { return 0; }
+  static int tiles_x(int w) { return (int)ceil_div(w, TS); }
+  static int tiles_y(int h) { return (int)ceil_div(h, TS); }
+  static __device__ __forceinline__ void tile(const BImg &im, const Args &a, int tx, int ty, unsigned char *) {
+    const int y = ty * TS + (int)(threadIdx.x >> 3);
+    const int x0 = tx * TS + (int)(threadIdx.x & 7) * 4;
+    if (y >= im.d.h || x0 >= im.d.w) return;
+    wp::PerArgs pa{};
+    wp::AffArgs aa{};
+    if constexpr (PERSP) {
+#pragma unroll
+      for (int i = 0; i < 9; i++) pa.m[i] = im.md[i];
+      pa.interp = a.interp;
+      pa.border = a.border;
+      pa.cv = im.cv;
+    } else {
+#pragma unroll
+      for (int i = 0; i < 6; i++) aa.m[i] = im.mf[i];
+      aa.interp = a.interp;
+      aa.border = a.border;
+      aa.cv = im.cv;
+    }
+    wp::warp4_u8<PERSP>(im.s, im.d, pa, aa, im.wide, x0, y);
+  }
+};
+
 // ----------------------------------------------------------- launching
 
 template <class Op>

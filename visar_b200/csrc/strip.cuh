@@ -387,7 +387,7 @@ struct GaussStrip {
   // fetched in order, one per call; rows past the top or bottom edge (a
   // warp-uniform case) are border-mapped, -1 being the constant fill. PRO:
   // the first rows of the queue, which hold every row above the image
-  // (R < kQD - 1); the later ones can only pass the bottom, by less than R
+  // (R < kGQ - 1); the later ones can only pass the bottom, by less than R
   // rows where it matters (j < nr), which the map below covers for images
   // taller than R.
   template <bool PRO>

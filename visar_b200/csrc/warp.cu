@@ -76,7 +76,7 @@ __global__ void __launch_bounds__(256) k_warp_persp(DImg s, DImg d, PerArgs a) {
   double sx = __dadd_rn(__dadd_rn(__dmul_rn(a.m[0], fx), __dmul_rn(a.m[1], fy)), a.m[2]);
   double sy = __dadd_rn(__dadd_rn(__dmul_rn(a.m[3], fx), __dmul_rn(a.m[4], fy)), a.m[5]);
   const double w = __dadd_rn(__dadd_rn(__dmul_rn(a.m[6], fx), __dmul_rn(a.m[7], fy)), a.m[8]);
-  const double iw = w != 0.0 ? __ddiv_rn(1.0, w) : 0.0;
+  const double iw = w != 0.0 ? __drcp_rn(w) : 0.0;  // correctly rounded: equals 1.0 / w
   sx = __dmul_rn(sx, iw);
   sy = __dmul_rn(sy, iw);
   T *o = row_ptr<T>(d, y) + (long long)x * cn;
@@ -139,6 +139,20 @@ __global__ void __launch_bounds__(256) k_warp_persp_c(DImg s, DImg d, PerArgs a,
   if (x < d.w && y < d.h) persp_px<T, CN>(s, d, a, wide, x, y);
 }
 
+// One-channel u8 INTER_LINEAR: 8 x 32 threads of 4 consecutive pixels each
+// (a block covers 32 x 32 output pixels, a warp 32 x 4).
+template <bool PERSP>
+__global__ void __launch_bounds__(256) k_warp4_u8(DImg s, DImg d, PerArgs pa, AffArgs aa, int wide) {
+  const int x0 = (blockIdx.x * 8 + threadIdx.x) * 4;
+  const int y = blockIdx.y * 32 + threadIdx.y;
+  if (x0 < d.w && y < d.h) warp4_u8<PERSP>(s, d, pa, aa, wide, x0, y);
+}
+
+// k_warp4_u8 applies: one-channel u8, INTER_LINEAR, 4-byte aligned destination rows.
+inline bool warp4_ok(const DImg &d, int interp, int cn, size_t tsize) {
+  return tsize == 1 && cn == 1 && interp != 0 && (uintptr_t)d.p % 4 == 0 && d.stride % 4 == 0;
+}
+
 template <class T>
 cudaError_t run_affine(const DImg &s, const DImg &d, const float m[6], int interp, int border, double value, cudaStream_t st) {
   AffArgs a;
@@ -149,6 +163,11 @@ cudaError_t run_affine(const DImg &s, const DImg &d, const float m[6], int inter
   const dim3 g2(ceil_div(d.w, 8), ceil_div(d.h, 32)), b2(8, 32);
   const int wide = ((uintptr_t)s.p % 8 == 0) && (s.stride % 8 == 0);
   const bool al4 = ((uintptr_t)s.p % 4 == 0) && (s.stride % 4 == 0);
+  if (warp4_ok(d, interp, d.cn, sizeof(T))) {
+    k_warp4_u8<false><<<dim3(ceil_div(d.w, 32), ceil_div(d.h, 32)), b2, 0, st>>>(s, d, PerArgs{}, a, wide);
+    note_launch();
+    return cudaGetLastError();
+  }
   switch (d.cn) {
     case 1: k_warp_affine_c<T, 1><<<g2, b2, 0, st>>>(s, d, a, wide); break;
     case 3: k_warp_affine_c<T, 3><<<g2, b2, 0, st>>>(s, d, a, wide); break;
@@ -174,6 +193,11 @@ cudaError_t run_persp(const DImg &s, const DImg &d, const double m[9], int inter
   const dim3 g2(ceil_div(d.w, 8), ceil_div(d.h, 32)), b2(8, 32);
   const int wide = ((uintptr_t)s.p % 8 == 0) && (s.stride % 8 == 0);
   const bool al4 = ((uintptr_t)s.p % 4 == 0) && (s.stride % 4 == 0);
+  if (warp4_ok(d, interp, d.cn, sizeof(T))) {
+    k_warp4_u8<true><<<dim3(ceil_div(d.w, 32), ceil_div(d.h, 32)), b2, 0, st>>>(s, d, a, AffArgs{}, wide);
+    note_launch();
+    return cudaGetLastError();
+  }
   switch (d.cn) {
     case 1: k_warp_persp_c<T, 1><<<g2, b2, 0, st>>>(s, d, a, wide); break;
     case 3: k_warp_persp_c<T, 3><<<g2, b2, 0, st>>>(s, d, a, wide); break;

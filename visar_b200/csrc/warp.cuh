@@ -177,7 +177,7 @@ __device__ __forceinline__ void persp_px(const DImg &s, const DImg &d, const Per
   double sx = __dadd_rn(__dadd_rn(__dmul_rn(a.m[0], fx), __dmul_rn(a.m[1], fy)), a.m[2]);
   double sy = __dadd_rn(__dadd_rn(__dmul_rn(a.m[3], fx), __dmul_rn(a.m[4], fy)), a.m[5]);
   const double w = __dadd_rn(__dadd_rn(__dmul_rn(a.m[6], fx), __dmul_rn(a.m[7], fy)), a.m[8]);
-  const double iw = w != 0.0 ? __ddiv_rn(1.0, w) : 0.0;
+  const double iw = w != 0.0 ? __drcp_rn(w) : 0.0;  // correctly rounded: equals 1.0 / w
   sx = __dmul_rn(sx, iw);
   sy = __dmul_rn(sy, iw);
   T *o = row_ptr<T>(d, y) + x * CN;
@@ -252,6 +252,117 @@ inline float sat_value_host(double v) {
     if (r <= (double)Lim<T>::lo) return (float)Lim<T>::lo;
     if (r >= (double)Lim<T>::hi) return (float)Lim<T>::hi;
     return (float)(int)r;
+  }
+}
+
+// Four consecutive pixels x0 .. x0 + 3 of row y of a one-channel u8 image,
+// INTER_LINEAR (the arithmetic of affine_px / persp_px): the coordinates of
+// all four first, then every tap load, then the blends, so that the four
+// pixels' loads are in flight together, and one 4-byte store (the
+// destination row at x0 is 4-byte aligned). Pixels whose taps leave the
+// source, or that lie past the row, take the per-pixel path.
+//
+// The fast path keeps conversions off the transcendental unit, with the
+// same values: a pixel's taps are inside exactly when 0 <= sx < w - 1 and
+// 0 <= sy < h - 1 (floor and the +-1e9 clamp change nothing there, and NaN
+// fails the test); floor(sx) is then sx + 2^52 rounded toward zero, less
+// 2^52 (2^23 in f32), exact below 2^52 (2^23), its low word the integer;
+// tap bytes become f32 as 2^23 + b - 2^23; x steps by exact adds.
+template <bool PERSP>
+__device__ __forceinline__ void warp4_u8(const DImg &s, const DImg &d, const PerArgs &pa, const AffArgs &aa, int wide,
+                                         int x0, int y) {
+  constexpr double kTwo52 = 4503599627370496.0;
+  constexpr float kTwo23 = 8388608.0f;
+  float ax[4], ay[4];
+  long long off[4];  // source offset of tap (ix, iy); -1: per-pixel path
+  float bx = 0.0f, by = 0.0f, xf0 = 0.0f;
+  double fx0 = 0.0, fy = 0.0;
+  if constexpr (PERSP) {
+    fx0 = (double)x0;
+    fy = (double)y;
+  } else {
+    const float yf = (float)y;
+    bx = __fadd_rn(__fmul_rn(aa.m[1], yf), aa.m[2]);
+    by = __fadd_rn(__fmul_rn(aa.m[4], yf), aa.m[5]);
+    xf0 = (float)x0;
+  }
+  // Inner bounds: below w - 1 (h - 1), and below the clamp (and 2^23 in f32).
+  const double limx = fmin((double)(s.w - 1), 1.0e9), limy = fmin((double)(s.h - 1), 1.0e9);
+  const float flimx = fminf((float)(s.w - 1), kTwo23), flimy = fminf((float)(s.h - 1), kTwo23);
+#pragma unroll
+  for (int p = 0; p < 4; p++) {
+    bool inner;
+    int ix, iy;
+    if constexpr (PERSP) {
+      const double fx = __dadd_rn(fx0, (double)p);
+      double sx = __dadd_rn(__dadd_rn(__dmul_rn(pa.m[0], fx), __dmul_rn(pa.m[1], fy)), pa.m[2]);
+      double sy = __dadd_rn(__dadd_rn(__dmul_rn(pa.m[3], fx), __dmul_rn(pa.m[4], fy)), pa.m[5]);
+      const double w = __dadd_rn(__dadd_rn(__dmul_rn(pa.m[6], fx), __dmul_rn(pa.m[7], fy)), pa.m[8]);
+      const double iw = w != 0.0 ? __drcp_rn(w) : 0.0;
+      sx = __dmul_rn(sx, iw);
+      sy = __dmul_rn(sy, iw);
+      inner = sx >= 0.0 && sy >= 0.0 && sx < limx && sy < limy;
+      const double tx = __dadd_rz(inner ? sx : 0.0, kTwo52), ty = __dadd_rz(inner ? sy : 0.0, kTwo52);
+      ix = (int)__double2loint(tx);
+      iy = (int)__double2loint(ty);
+      ax[p] = (float)__dsub_rn(sx, __dsub_rn(tx, kTwo52));
+      ay[p] = (float)__dsub_rn(sy, __dsub_rn(ty, kTwo52));
+    } else {
+      const float xf = __fadd_rn(xf0, (float)p);
+      const float sx = fmaf(aa.m[0], xf, bx), sy = fmaf(aa.m[3], xf, by);
+      inner = sx >= 0.0f && sy >= 0.0f && sx < flimx && sy < flimy;
+      const float tx = __fadd_rz(inner ? sx : 0.0f, kTwo23), ty = __fadd_rz(inner ? sy : 0.0f, kTwo23);
+      ix = (int)(__float_as_uint(tx) & 0x7FFFFFu);
+      iy = (int)(__float_as_uint(ty) & 0x7FFFFFu);
+      ax[p] = __fsub_rn(sx, __fsub_rn(tx, kTwo23));
+      ay[p] = __fsub_rn(sy, __fsub_rn(ty, kTwo23));
+    }
+    off[p] = inner && x0 + p < d.w ? (long long)iy * s.stride + ix : -1;
+  }
+  float v[4][4];
+#pragma unroll
+  for (int p = 0; p < 4; p++) {
+    const uint8_t *r = s.p + (off[p] < 0 ? 0 : off[p]);  // in bounds either way
+    v[p][0] = __fsub_rn(__uint_as_float(0x4B000000u | __ldg(r)), kTwo23);
+    v[p][1] = __fsub_rn(__uint_as_float(0x4B000000u | __ldg(r + 1)), kTwo23);
+    v[p][2] = __fsub_rn(__uint_as_float(0x4B000000u | __ldg(r + s.stride)), kTwo23);
+    v[p][3] = __fsub_rn(__uint_as_float(0x4B000000u | __ldg(r + s.stride + 1)), kTwo23);
+  }
+  uint32_t out = 0;
+#pragma unroll
+  for (int p = 0; p < 4; p++) {
+    float val;
+    if constexpr (PERSP) {
+      const float one_ax = __fsub_rn(1.0f, ax[p]), one_ay = __fsub_rn(1.0f, ay[p]);
+      float acc = 0.0f;
+      acc = __fadd_rn(acc, __fmul_rn(v[p][0], __fmul_rn(one_ax, one_ay)));
+      acc = __fadd_rn(acc, __fmul_rn(v[p][1], __fmul_rn(ax[p], one_ay)));
+      acc = __fadd_rn(acc, __fmul_rn(v[p][2], __fmul_rn(one_ax, ay[p])));
+      acc = __fadd_rn(acc, __fmul_rn(v[p][3], __fmul_rn(ax[p], ay[p])));
+      val = acc;
+    } else {
+      const float v0 = fmaf(ax[p], __fsub_rn(v[p][1], v[p][0]), v[p][0]);
+      const float v1 = fmaf(ax[p], __fsub_rn(v[p][3], v[p][2]), v[p][2]);
+      val = fmaf(ay[p], __fsub_rn(v1, v0), v0);
+    }
+    out |= (uint32_t)round_u8(val) << (8 * p);
+  }
+  uint8_t *o = row_ptr<uint8_t>(d, y) + x0;
+  const unsigned fast = (off[0] >= 0 ? 1u : 0u) | (off[1] >= 0 ? 2u : 0u) | (off[2] >= 0 ? 4u : 0u) | (off[3] >= 0 ? 8u : 0u);
+  if (fast == 15u) {
+    *reinterpret_cast<uint32_t *>(o) = out;
+    return;
+  }
+  const int np = min(4, d.w - x0);
+#pragma unroll 1
+  for (int p = 0; p < np; p++) {
+    if ((fast >> p) & 1u) {
+      o[p] = (uint8_t)(out >> (8 * p));
+    } else if constexpr (PERSP) {
+      persp_px<uint8_t, 1>(s, d, pa, wide, x0 + p, y);
+    } else {
+      affine_px<uint8_t, 1>(s, d, aa, wide, x0 + p, y);
+    }
   }
 }
 
