@@ -889,6 +889,7 @@ def bench_served(args, ctx):
                 row["launches"] = st["launches"]
                 row["fallback_calls"] = st["fallback_calls"]
                 row["deferred"] = st["deferred"]
+                row["solo"] = st["solo"]
         results.append(row)
     clk.__exit__(None, None, None)
     clocks = clk.summary()

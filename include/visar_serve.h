@@ -34,7 +34,7 @@ typedef struct visar_server_config {
     size_t pool_bytes;   /* device pool for intermediate and final results (0: 64 GiB) */
     int mode;            /* enum visar_serve_mode */
     int max_inflight;    /* scheduling rounds queued on the GPU at once (0: 4) */
-    int streams;         /* streams the rounds alternate over (0: 2) */
+    int streams;         /* streams the stage groups of a round spread over (0: 4) */
 } visar_server_config;
 
 typedef struct visar_server visar_server;
@@ -47,6 +47,8 @@ typedef struct visar_server_stats {
     size_t pool_bytes, pool_used, pool_reserved;
     double mean_batch;        /* requests per stage group */
     uint64_t deferred;        /* stage groups put off to a later round for pool or staging memory */
+    uint64_t solo;            /* requests run whole through the per-call entry points: new, with no
+                                 request sharing their first stage (a round would run them alone) */
 } visar_server_stats;
 
 int visar_server_create(const visar_server_config *cfg, visar_server **out);

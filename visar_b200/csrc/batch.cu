@@ -341,21 +341,24 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
     if (m) std::memcpy(f.m, m, sizeof(double) * (st.kind == VISAR_STAGE_WARP_AFFINE ? 6 : 9));
     step.fallbacks.push_back(f);
   };
-  // u8 inputs whose rows are not 8-byte aligned (caller-owned images) are
-  // first copied, in one batched launch, into pitched pool images, so the
-  // stencil classes that need aligned rows take them instead of the per-call
-  // fallback.
+  // u8 inputs whose rows are not 8-byte aligned and f32 inputs whose rows are
+  // not 16-byte aligned (caller-owned images) are first copied, in one
+  // batched launch, into pitched pool images, so the stencil classes that
+  // need aligned rows take them instead of the per-call fallback.
   std::vector<Buf> src(cur.begin(), cur.end());
   auto repack_unaligned = [&]() -> int {
     for (size_t i = 0; i < n; i++) {
       const Buf &im = cur[i];
-      if (im.depth != k8U || u8_aligned8(im.v) || im.v.w < 2 || im.v.h < 2) continue;
+      // u8 rows that are not 8-byte aligned (strips), f32 rows that are not
+      // 16-byte aligned (band kernels).
+      const bool unaligned = im.depth == k8U ? !u8_aligned8(im.v) : im.depth == k32F && !aligned16(im.v);
+      if (!unaligned || im.v.w < 2 || im.v.h < 2) continue;
       if (im.v.cn != 1 && im.v.cn != 3 && im.v.cn != 4) continue;
       Buf t;
       if (!B.image(im.v.w, im.v.h, im.v.cn, im.depth, t)) return VISAR_OUT_OF_MEMORY;
       Launch *l = class_of(ls, kOpCopy, im.depth, im.v.cn, 0, false);
       add_img(l, bimg(im.v, t.v), im.input);
-      u8_bytes(*l, im.v, t.v, 1);
+      u8_bytes(*l, im.v, t.v, depth_size(im.depth));
       src[i] = t;
     }
     for (Launch &l : ls) {

@@ -182,7 +182,11 @@ struct Trace {
 };
 
 struct Round {
+  // ev_launch: every launch of the round is done (each stage group runs on
+  // a stream of its own and records a group event, in groups); ev_fb: its
+  // per-call fallbacks are.
   cudaEvent_t ev_launch = nullptr, ev_fb = nullptr;
+  std::vector<cudaEvent_t> groups;
   std::vector<void *> blocks;           // pool blocks freed when the round is done
   std::vector<uint64_t> finishing;      // requests whose last stage ran here
   size_t staging = 0, staging_end = 0;  // staging the round consumed, ring position after it
@@ -323,6 +327,7 @@ struct visar_server {
     for (Round &r : rounds) {
       free_events.push_back(r.ev_launch);
       free_events.push_back(r.ev_fb);
+      free_events.insert(free_events.end(), r.groups.begin(), r.groups.end());
     }
     rounds.clear();
     incoming.clear();
@@ -370,10 +375,13 @@ struct visar_server {
       for (uint64_t id : r.finishing) finished(id, t);
       for (auto &kv : reqs) {
         Req &q = *kv.second;
-        if (q.ready == r.ev_launch || q.ready == r.ev_fb) q.ready = nullptr;
+        if (q.ready == r.ev_launch || q.ready == r.ev_fb ||
+            std::find(r.groups.begin(), r.groups.end(), q.ready) != r.groups.end())
+          q.ready = nullptr;
       }
       free_events.push_back(r.ev_launch);
       free_events.push_back(r.ev_fb);
+      free_events.insert(free_events.end(), r.groups.begin(), r.groups.end());
       rounds.pop_front();
       cv_done.notify_all();
     }
@@ -420,7 +428,9 @@ struct visar_server {
   }
 
   // One scheduling round: every admitted request advances one stage, in
-  // groups of equal stages. Returns false when there was nothing to do.
+  // groups of equal stages. Each group runs on a stream of its own after the
+  // rounds that produced its inputs, so independent groups overlap on the
+  // GPU. Returns false when there was nothing to do.
   bool launch_round() {
     if (admitted.empty()) return false;
     std::map<std::string, std::vector<uint64_t>> groups_by;
@@ -432,6 +442,7 @@ struct visar_server {
     rd.ev_launch = get_event();
     rd.ev_fb = get_event();
     const cudaStream_t ls = streams[next_stream];
+    int gstream = next_stream;
     next_stream = (next_stream + 1) % (int)streams.size();
     const cudaStream_t old = thread_stream();
     const int old_async = thread_async();
@@ -507,20 +518,23 @@ struct visar_server {
         if (reqs[id]->ready) waits.push_back(reqs[id]->ready);
       std::sort(waits.begin(), waits.end());
       waits.erase(std::unique(waits.begin(), waits.end()), waits.end());
+      cudaEvent_t gev = nullptr;
       if (!step.launches.empty()) {
-        for (cudaEvent_t e : waits) cudaStreamWaitEvent(ls, e, 0);
+        const cudaStream_t gs = streams[gstream];
+        gstream = (gstream + 1) % (int)streams.size();
+        for (cudaEvent_t e : waits) cudaStreamWaitEvent(gs, e, 0);
         size_t off = 0;
         for (const Builder::Upload &u : B.uploads) {
           std::memcpy(stg + off, u.data.data(), u.data.size());
-          cudaMemcpyAsync(u.dst, stg + off, u.data.size(), cudaMemcpyHostToDevice, ls);
+          cudaMemcpyAsync(u.dst, stg + off, u.data.size(), cudaMemcpyHostToDevice, gs);
           off += (u.data.size() + 255) & ~(size_t)255;
         }
         for (size_t j = 0; j < step.launches.size(); j++) {
           Launch &L = step.launches[j];
-          cudaMemsetAsync(counters[j], 0, sizeof(int), ls);
+          cudaMemsetAsync(counters[j], 0, sizeof(int), gs);
           ctx.counters = counters[j];
           L.counter = 0;
-          const cudaError_t le = run_launch(ctx, L, ls);
+          const cudaError_t le = run_launch(ctx, L, gs);
           stats.launches++;
           if (le != cudaSuccess) {
             cuda_status(le);
@@ -533,6 +547,10 @@ struct visar_server {
             }
           }
         }
+        gev = get_event();
+        cudaEventRecord(gev, gs);
+        cudaStreamWaitEvent(ls, gev, 0);
+        rd.groups.push_back(gev);
       } else if (!B.uploads.empty()) {
         size_t off = 0;
         for (const Builder::Upload &u : B.uploads) {
@@ -572,7 +590,7 @@ struct visar_server {
           q.cur_owned = true;
           outs.push_back(next[i].v.p);
         }
-        q.ready = fell_back ? rd.ev_fb : rd.ev_launch;
+        q.ready = fell_back ? rd.ev_fb : gev ? gev : rd.ev_launch;
         q.next++;
         advanced.push_back(ids[i]);
         if (q.next == (int)q.st.size()) rd.finishing.push_back(ids[i]);
@@ -585,6 +603,7 @@ struct visar_server {
     if (advanced.empty()) {
       free_events.push_back(rd.ev_launch);
       free_events.push_back(rd.ev_fb);
+      free_events.insert(free_events.end(), rd.groups.begin(), rd.groups.end());
       return false;
     }
     cudaEventRecord(rd.ev_launch, ls);
@@ -599,8 +618,25 @@ struct visar_server {
     return true;
   }
 
-  // Plain mode: each admitted request runs all its stages now, call by call.
-  bool launch_plain() {
+  // True when every admitted request is new (no stage run yet) and no two of
+  // them share a first stage: a scheduling round would run each alone, so
+  // the per-call path (less host work per stage, no round events) serves
+  // them sooner.
+  bool solo() {
+    if (admitted.empty()) return false;
+    std::vector<std::string> keys;
+    for (uint64_t id : admitted) {
+      const Req &q = *reqs[id];
+      if (q.next != 0 || q.ready) return false;
+      keys.push_back(stage_key(q.st[0]));
+    }
+    std::sort(keys.begin(), keys.end());
+    return std::adjacent_find(keys.begin(), keys.end()) == keys.end();
+  }
+
+  // Plain mode (and solo requests): each admitted request runs all its
+  // stages now, call by call.
+  bool launch_plain(bool solo_reqs = false) {
     if (admitted.empty()) return false;
     Round rd;
     rd.ev_launch = get_event();
@@ -634,7 +670,7 @@ struct visar_server {
         std::memset(f.m, 0, sizeof(f.m));
         std::copy(q.mats[k].begin(), q.mats[k].end(), f.m);
         const int rc = run_fallback(f);
-        stats.fallback_calls++;
+        if (!solo_reqs) stats.fallback_calls++;
         if (q.cur_owned) rd.blocks.push_back(q.cur.v.p);
         q.cur = f.d;
         q.cur_owned = true;
@@ -646,6 +682,11 @@ struct visar_server {
       }
       q.next = (int)q.st.size();
       rd.finishing.push_back(id);
+      if (solo_reqs) {
+        stats.solo++;
+        groups++;
+        grouped++;
+      }
     }
     set_thread_stream(old, old_async);
     admitted.clear();
@@ -666,8 +707,11 @@ struct visar_server {
         if (!broken.empty() && !incoming.empty()) fail_all(cudaSuccess);
         poll_rounds();
         admit();
-        if (broken.empty() && (int)rounds.size() < cfg.max_inflight)
-          did = cfg.mode == VISAR_SERVE_PLAIN ? launch_plain() : launch_round();
+        if (broken.empty() && (int)rounds.size() < cfg.max_inflight) {
+          if (cfg.mode == VISAR_SERVE_PLAIN) did = launch_plain();
+          else if (incoming.empty() && solo()) did = launch_plain(true);
+          else did = launch_round();
+        }
       }
       if (!did) std::this_thread::sleep_for(std::chrono::microseconds(20));
     }
@@ -684,7 +728,7 @@ int visar_server_create(const visar_server_config *cfg, visar_server **out) {
   if (cfg) s->cfg = *cfg;
   if (s->cfg.pool_bytes == 0) s->cfg.pool_bytes = (size_t)64 << 30;
   if (s->cfg.max_inflight <= 0) s->cfg.max_inflight = 4;
-  if (s->cfg.streams <= 0) s->cfg.streams = 2;
+  if (s->cfg.streams <= 0) s->cfg.streams = 4;
   if (s->cfg.mode != VISAR_SERVE_BATCHED && s->cfg.mode != VISAR_SERVE_PLAIN)
     return report_error(VISAR_INVALID_ARGUMENT, "InvalidArgument: serve mode");
   cudaError_t e = cudaGetDevice(&s->dev);
@@ -832,6 +876,7 @@ void visar_server_destroy(visar_server *s) {
   for (Round &r : s->rounds) {
     s->free_events.push_back(r.ev_launch);
     s->free_events.push_back(r.ev_fb);
+    s->free_events.insert(s->free_events.end(), r.groups.begin(), r.groups.end());
   }
   for (cudaEvent_t e : s->free_events) cudaEventDestroy(e);
   delete s;
