@@ -630,7 +630,7 @@ def bench_video(args, ctx):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(ctx.stream)
     for k in range(p_n):
-        video_plain(vb, frames[k], outs)
+        video_plain(vb, frames[k % V_FRAMES], outs)
     e1.record(ctx.stream)
     torch.cuda.synchronize()
     p_ms = ctx.max_over_ranks(e0.elapsed_time(e1))
@@ -640,7 +640,7 @@ def bench_video(args, ctx):
     plan.profile(True)
     per = {}
     for r in range(6):
-        plan.set_input(0, frames[r])
+        plan.set_input(0, frames[r % V_FRAMES])
         plan.run()
         torch.cuda.synchronize()
         if r == 0:
@@ -659,7 +659,7 @@ def bench_video(args, ctx):
     hosts = []
     for k in range(nh):
         h = torch.empty((V_H, V_W, 3), dtype=torch.uint8, pin_memory=True).numpy()
-        h[...] = frames[k].cpu().numpy()
+        h[...] = frames[k % V_FRAMES].cpu().numpy()
         hosts.append(h)
     houts = [torch.empty((V_H, V_W), dtype=torch.uint8, pin_memory=True).numpy() for _ in range(V_INSTANCES)]
     # Each instance's own input buffer receives its uploads; instance i's
@@ -696,7 +696,7 @@ def bench_video(args, ctx):
     cpu, parity = None, None
     if ctx.rank == 0 and ctx.world == 1 and not args.no_cpu_baseline:
         nchk = 4
-        xs = [frames[k].cpu().numpy() for k in range(8)]
+        xs = [frames[k % V_FRAMES].cpu().numpy() for k in range(8)]
         n, dt, cores, ref = oracle_run(video_oracle, xs, 0, 8.0, keep=True)
         n1, dt1, _, _ = oracle_run(video_oracle, xs, 1, 8.0)
         cpu = {"value": n * V_W * V_H / dt / 1e9, "unit": "Gpix/s", "cores": cores, "kind": "port",
@@ -706,7 +706,7 @@ def bench_video(args, ctx):
                "cv2_context": cv2_context(cv2_video_frame, xs, lambda x: V_W * V_H, 5.0)}
         good = 0
         for k in range(min(nchk, len(ref))):
-            plan.set_input(0, frames[k])
+            plan.set_input(0, frames[k % V_FRAMES])
             plan.run()
             torch.cuda.synchronize()
             good += bool(np.array_equal(plan.output(0).cpu().numpy(), ref[k]))
@@ -1410,9 +1410,13 @@ def main():
     ap.add_argument("--duration", type=float, default=20.0, help="seconds per arrival rate (served workload)")
     ap.add_argument("--images", type=int, default=0,
                     help="batched-mixed: the first N images only (a reduced plan for profiler captures; not a bench line)")
+    ap.add_argument("--frames", type=int, default=0,
+                    help="video-4k: N frames in HBM instead of 300 (a reduced case for profiler captures; not a bench line)")
     args = ap.parse_args()
-    global IMAGE_LIMIT
+    global IMAGE_LIMIT, V_FRAMES
     IMAGE_LIMIT = max(0, args.images)
+    if args.frames > 0:
+        V_FRAMES = args.frames
     ours, ref = WORKLOADS[args.workload]
     subs = args.workload == "batched-mixed" and not args.only and args.gpus == 1
     if args.impl == "reference":

@@ -90,7 +90,9 @@ void visar_batch_destroy(visar_batch *b);
 
 /* Points input i at another device image of the same width, height,
    channels, depth, row stride and at least the same alignment (e.g. the next
-   video frame). Enqueued on the run stream (a one-thread kernel patches the
+   video frame). As with plan-owned inputs, kernels may read every row of it,
+   the last one included, up to its length rounded up to 8 bytes (within the
+   stride). Enqueued on the run stream (a one-thread kernel patches the
    device descriptors), so graph replays see it. */
 int visar_batch_set_input(visar_batch *b, size_t i, const visar_image *img);
 /* Host <-> device copies of all inputs / final outputs, from or to `host[i]`,

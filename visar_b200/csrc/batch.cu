@@ -346,12 +346,17 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
   // batched launch, into pitched pool images, so the stencil classes that
   // need aligned rows take them instead of the per-call fallback.
   std::vector<Buf> src(cur.begin(), cur.end());
-  auto repack_unaligned = [&]() -> int {
+  // ragged: also u8 images of the caller whose rows are not a multiple of 8
+  // bytes (the Gaussian strips read rows up to that rounding; plan images are
+  // padded to it).
+  auto repack_unaligned = [&](bool ragged = false) -> int {
     for (size_t i = 0; i < n; i++) {
       const Buf &im = cur[i];
       // u8 rows that are not 8-byte aligned (strips), f32 rows that are not
       // 16-byte aligned (band kernels).
-      const bool unaligned = im.depth == k8U ? !u8_aligned8(im.v) : im.depth == k32F && !aligned16(im.v);
+      const bool unaligned =
+          im.depth == k8U ? !u8_aligned8(im.v) || (ragged && !im.padded && ((long long)im.v.w * im.v.cn) % 8 != 0)
+                          : im.depth == k32F && !aligned16(im.v);
       if (!unaligned || im.v.w < 2 || im.v.h < 2) continue;
       if (im.v.cn != 1 && im.v.cn != 3 && im.v.cn != 4) continue;
       Buf t;
@@ -393,7 +398,7 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
       const double sx = st.d[0], sy = st.d[1] > 0 ? st.d[1] : st.d[0];
       if (border < 0 || border > 4) return VISAR_UNSUPPORTED;
       if (kw_in < 0 || kh_in < 0) return VISAR_INVALID_ARGUMENT;
-      if (const int rc = repack_unaligned(); rc != VISAR_OK) return rc;
+      if (const int rc = repack_unaligned(true); rc != VISAR_OK) return rc;
       for (size_t i = 0; i < n; i++) {
         const Buf &im = src[i];
         if (!B.image(im.v.w, im.v.h, im.v.cn, im.depth, next[i])) return VISAR_OUT_OF_MEMORY;
@@ -437,15 +442,14 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
           std::vector<int64_t> t(kw);
           gaussian_kernel_fixed(t.data(), kw, sx, 8);
           // Strips map rows past the bottom edge in closed form (images taller
-          // than the radius) and take border columns from their own row
-          // window (not the far end of the row: no wrap); they write whole
-          // 8-byte words into padded destination rows.
-          if (binomial_taps(t) && u8_aligned8(im.v) && im.v.h > kw / 2 && border != kWrap && next[i].padded) {
+          // than the radius), take border columns from their own row window
+          // (not the far end of the row: no wrap), and read and write whole
+          // 8-byte words (padded rows or rows of 8-byte multiples).
+          const bool words = im.padded || ((long long)im.v.w * im.v.cn) % 8 == 0;
+          if (binomial_taps(t) && u8_aligned8(im.v) && im.v.h > kw / 2 && border != kWrap && next[i].padded && words) {
             Launch *l = class_of(ls, kOpGaussStrip, k8U, im.v.cn, kw, false);
             l->border = border;
-            BImg b = bimg(im.v, next[i].v);
-            b.pad = (im.padded && im.input < 0 ? 1 : 0) | 2;
-            add_img(l, b, im.input);
+            add_img(l, bimg(im.v, next[i].v), im.input);
             u8_bytes(*l, im.v, next[i].v, 1);
             continue;
           }
@@ -498,7 +502,7 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
           mode[i] = 2;
           Launch *l = class_of(ls, kOpMorphStrip, k8U, im.v.cn, kh, op == 3, true, prof);
           BImg b = bimg(im.v, next[i].v);
-          b.pad = (im.padded && im.input < 0 ? 1 : 0) | (next[i].padded ? 2 : 0);
+          b.pad = (im.padded ? 1 : 0) | (next[i].padded ? 2 : 0);
           add_img(l, b, im.input);
           u8_bytes(*l, im.v, next[i].v, 1);
           continue;
@@ -528,7 +532,7 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
           const Buf &im = src[i];
           const DImg from = p == 0 ? im.v : tmp[i][(p - 1) % 2].v;
           const DImg dst = p + 1 == np ? next[i].v : tmp[i][p % 2].v;
-          const bool from_pad = p == 0 ? im.padded && im.input < 0 : true;
+          const bool from_pad = p == 0 ? im.padded : true;
           Launch *l;
           if (mode[i] == 1) {
             l = class_of(pl, kOpMorphStrip, k8U, im.v.cn, kh, passes[p], false, prof);

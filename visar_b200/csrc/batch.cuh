@@ -712,7 +712,7 @@ struct OpGaussStrip {
   using Args = strip::GaussArgs;
   static size_t smem(const Args &) { return 0; }
   static __device__ __forceinline__ void tile(const BImg &im, const Args &a, int tx, int ty, int lane) {
-    strip::gauss_strip<K, CN, RH>(im.s, im.d, a.border, im.pad, tx, ty, lane);
+    strip::gauss_strip<K, CN, RH>(im.s, im.d, a.border, tx, ty, lane);
   }
 };
 

@@ -728,7 +728,7 @@ int visar_server_create(const visar_server_config *cfg, visar_server **out) {
   if (cfg) s->cfg = *cfg;
   if (s->cfg.pool_bytes == 0) s->cfg.pool_bytes = (size_t)64 << 30;
   if (s->cfg.max_inflight <= 0) s->cfg.max_inflight = 4;
-  if (s->cfg.streams <= 0) s->cfg.streams = 4;
+  if (s->cfg.streams <= 0) s->cfg.streams = 8;
   if (s->cfg.mode != VISAR_SERVE_BATCHED && s->cfg.mode != VISAR_SERVE_PLAIN)
     return report_error(VISAR_INVALID_ARGUMENT, "InvalidArgument: serve mode");
   cudaError_t e = cudaGetDevice(&s->dev);

@@ -238,9 +238,9 @@ __device__ __forceinline__ void st_global8_if(uint8_t *g, uint2 v, bool p) {
 // F = 2^(8-SH) equals (H + 2^(SH-1)) >> SH.
 //
 // Lanes that start inside the row copy 8 bytes of it into their slot of the
-// row queue (the source rows are readable up to their length rounded up to 8
-// samples, except the last row of an unpadded image, whose end is read
-// bytewise) and the others fill theirs; each lane then takes its samples
+// row queue (source rows are readable up to their length rounded up to 8
+// samples: rows of 8-sample multiples, or padded images, which the plan
+// guarantees) and the others fill theirs; each lane then takes its samples
 // from a 16-byte window of the warp's slot, byte k from window byte u_k,
 // three byte permutes per 4-byte word (in a row's inner strips the window
 // holds the lane's own bytes, unpermuted). Samples outside
@@ -290,7 +290,8 @@ struct GaussStrip {
   static constexpr int QD = kGQ - 1;  // rows in flight
 
   const DImg s, d;  // copies (kept in registers across the row loop)
-  int border, pad, H, first, nr, ylim, yout;
+  int border, H, first, nr, ylim, yout;
+  int bA, bS;  // rows sy >= H map to bA - bS * sy (-1: constant fill)
   long long n, gs;
   bool out_lane, from;
   GaussQueue q;
@@ -301,15 +302,20 @@ struct GaussStrip {
   uint32_t ca[K - 1][4], cb[K - 1][4];
   int woff;  // window offset from this lane's slot
 
-  __device__ __forceinline__ GaussStrip(const DImg &s_, const DImg &d_, int border_, int pad_, int tx, int ty,
-                                        int lane)
-      : s(s_), d(d_), border(border_), pad(pad_) {
+  __device__ __forceinline__ GaussStrip(const DImg &s_, const DImg &d_, int border_, int tx, int ty, int lane)
+      : s(s_), d(d_), border(border_) {
     n = (long long)s.w * CN;
     gs = ((long long)tx * G::OL - HALO + lane) * kSPL;
     out_lane = lane >= HALO && lane < 32 - HALO && gs < n;
     from = gs >= 0 && gs < n;
     q = gauss_queue(lane);
     H = s.h;
+    // border.map just below the image (rows H .. H + R - 1 where it matters):
+    // replicate H - 1, reflect 2H - 1 - sy, reflect-101 2H - 2 - sy, wrap
+    // sy - H, constant the fill (images are taller than R).
+    bA = border == kReplicate ? H - 1 : border == kReflect ? 2 * H - 1 : border == kReflect101 ? 2 * H - 2
+         : border == kWrap ? -H : -1;
+    bS = border == kReflect || border == kReflect101 ? 1 : border == kWrap ? -1 : 0;
     const int y0 = ty * RH;
     first = y0 - R;
     // Only the rows the tile's outputs (y < h) need: at most R past the image.
@@ -341,6 +347,17 @@ struct GaussStrip {
   }
 
   __device__ __forceinline__ void edge_setup(int lane) {
+    if (__all_sync(kFull, gs >= 0 && gs + kSPL <= n)) {
+      // Inner strip: the lane's own bytes (lane 31's window starts a word
+      // earlier).
+      const bool last = lane * kSPL > 256 - 16;
+      woff = last ? -kSPL : 0;
+      const uint32_t a0 = last ? 0u : 0x3210u, b0 = last ? 0x3210u : 0u, m0 = last ? 0x7654u : 0x3210u;
+      const uint32_t a1 = last ? 0u : 0x7654u, b1 = last ? 0x7654u : 0u;
+      st_shared16(q.par, make_uint4(a0, b0, m0, a1));
+      st_shared16(q.par + 16, make_uint4(b1, m0, ~0u, ~0u));
+      return;
+    }
     const long long base = gs - (long long)lane * kSPL;  // the strip's first sample
     const long long need_lo = base + kSPL * HALO - G::REACH;
     const long long need_hi = min(base + kSPL * (32 - HALO), n) + G::REACH;
@@ -374,52 +391,20 @@ struct GaussStrip {
     st_shared16(q.par + 16, make_uint4(sb[1], sm[1], (uint32_t)keep, (uint32_t)(keep >> 32)));
   }
 
-  // The row end of the last row of an unpadded image (cnt < 8 bytes), bytewise.
-  static __device__ __forceinline__ uint2 load_row_end(const uint8_t *p, int cnt) {
-    uint32_t v[2] = {0, 0};
-#pragma unroll
-    for (int k = 0; k < kSPL; k++)
-      if (k < cnt) v[k >> 2] |= (uint32_t)__ldg(p + k) << (8 * (k & 3));
-    return make_uint2(v[0], v[1]);
-  }
-
   // Source row j into its slot (rows j >= nr: nothing is read). Rows are
-  // fetched in order, one per call; rows past the top or bottom edge (a
-  // warp-uniform case) are border-mapped, -1 being the constant fill. PRO:
-  // the first rows of the queue, which hold every row above the image
-  // (R < kGQ - 1); the later ones can only pass the bottom, by less than R
-  // rows where it matters (j < nr), which the map below covers for images
-  // taller than R.
+  // fetched in order, one per call. PRO: the first rows of the queue, which
+  // hold every row above the image (R < kGQ - 1), border-mapped in full; the
+  // later ones can only pass the bottom, by less than R rows where it
+  // matters (j < nr), mapped in closed form (bA, bS) without branches.
   template <bool PRO>
   __device__ __forceinline__ void fetch(int j) {
     const int sy = first + j;
-    const uint8_t *p = fp;
+    int my;
+    if constexpr (PRO) my = (unsigned)sy < (unsigned)H ? sy : border_map(sy, H, border);
+    else my = sy < H ? sy : bA - bS * sy;
+    const bool ok = j < nr && (unsigned)my < (unsigned)H && from;
+    fetch8_inside(q.slot(j), fp + (long long)(my - sy) * s.stride, ok, 0u);
     fp += s.stride;
-    bool ok = j < nr;
-    int my = sy;
-    if constexpr (PRO) {
-      if ((unsigned)sy >= (unsigned)H) {
-        my = border_map(sy, H, border);
-        ok = ok && my >= 0;
-        p += (long long)(my - sy) * s.stride;
-      }
-    } else {
-      if (sy >= H) {
-        my = border == kReplicate    ? H - 1
-             : border == kReflect    ? 2 * H - 1 - sy
-             : border == kReflect101 ? 2 * H - 2 - sy
-             : border == kWrap       ? sy - H
-                                     : -1;
-        ok = ok && (unsigned)my < (unsigned)H;
-        p += (long long)(my - sy) * s.stride;
-      }
-    }
-    // Lanes starting inside the row copy 8 bytes; a lane straddling the end
-    // of an unpadded image's last row reads the row end bytewise.
-    if (!(pad & 1) && my == H - 1 && from && gs + kSPL > n)
-      st_shared8(q.slot(j), ok ? load_row_end(p, (int)(n - gs)) : make_uint2(0, 0));
-    else
-      fetch8_inside(q.slot(j), p, ok && from, 0u);
   }
 
   // This lane's 8 samples of row j from its window of the slot.
@@ -441,8 +426,9 @@ struct GaussStrip {
     yout++;
   }
 
-  // Source row j; the output row j - (K - 1) once the cascade is full.
-  template <bool ODD>
+  // Source row j; OUT: the cascade is full (j >= K - 1) and output row
+  // j - (K - 1) is computed.
+  template <bool ODD, bool OUT>
   __device__ __forceinline__ void step(int j) {
     const uint32_t(&in)[K - 1][4] = ODD ? cb : ca;
     uint32_t(&out)[K - 1][4] = ODD ? ca : cb;
@@ -463,7 +449,7 @@ struct GaussStrip {
         out[a][i] = v[i];
         v[i] = t;
       }
-    if (j < K - 1) return;
+    if constexpr (!OUT) return;
     Window<HALO, -G::REACH, kSPL - 1 + G::REACH> win;
     win.gather(v);
     uint32_t h[4];
@@ -496,22 +482,26 @@ struct GaussStrip {
     for (int a = 0; a < K - 1; a++)
 #pragma unroll
       for (int i = 0; i < 4; i++) ca[a][i] = 0;
+    static_assert((K - 1) % 2 == 0, "the cascade fills in pairs of rows");
+#pragma unroll 1
+    for (int j = 0; j < K - 1; j += 2) {
+      step<false, false>(j);
+      step<true, false>(j + 1);
+    }
     // Pairs of rows; rows past nr are neither read nor stored.
 #pragma unroll 1
-    for (int j = 0; j < nr; j += 2) {
-      step<false>(j);
-      step<true>(j + 1);
+    for (int j = K - 1; j < nr; j += 2) {
+      step<false, true>(j);
+      step<true, true>(j + 1);
     }
   }
 };
 
-// pad: bit 0 = source rows readable up to their length rounded up to 8
-// samples (all but the last row always are: strips take 8-byte aligned rows),
-// bit 1 = the same for destination rows, which the strip requires.
+// The plan hands the strip source and destination rows that are readable
+// and writable up to their length rounded up to 8 samples.
 template <int K, int CN, int RH>
-__device__ __forceinline__ void gauss_strip(const DImg &s, const DImg &d, int border, int pad, int tx, int ty,
-                                            int lane) {
-  GaussStrip<K, CN, RH> g(s, d, border, pad, tx, ty, lane);
+__device__ __forceinline__ void gauss_strip(const DImg &s, const DImg &d, int border, int tx, int ty, int lane) {
+  GaussStrip<K, CN, RH> g(s, d, border, tx, ty, lane);
   g.rows(lane);
 }
 
