@@ -347,8 +347,8 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
   // need aligned rows take them instead of the per-call fallback.
   std::vector<Buf> src(cur.begin(), cur.end());
   // ragged: also u8 images of the caller whose rows are not a multiple of 8
-  // bytes (the Gaussian strips read rows up to that rounding; plan images are
-  // padded to it).
+  // bytes (the strips read rows up to that rounding; plan images are padded
+  // to it).
   auto repack_unaligned = [&](bool ragged = false) -> int {
     for (size_t i = 0; i < n; i++) {
       const Buf &im = cur[i];
@@ -489,7 +489,7 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
       std::vector<int> mode(n, 0);  // 0 fallback, 1 strip passes, 2 fused strip, 3 band passes, 4 f32 rectangle passes
       const bool rect = std::all_of(mask.begin(), mask.end(), [](uint8_t m) { return m != 0; });
       if (kernel_ok) {
-        if (const int rc = repack_unaligned(); rc != VISAR_OK) return rc;
+        if (const int rc = repack_unaligned(true); rc != VISAR_OK) return rc;
       }
       for (size_t i = 0; i < n; i++) {
         const Buf &im = src[i];
@@ -497,13 +497,14 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
         const bool u8ok = kernel_ok && im.depth == k8U && (im.v.cn == 1 || im.v.cn == 3 || im.v.cn == 4) &&
                           u8_aligned4(im.v);
         fast::MFArgs ma;
-        const bool strip_ok = u8ok && prof < strip::kProfileCount && u8_aligned8(im.v);
+        // Strips read and write whole 8-byte words (padded rows or rows of
+        // 8-byte multiples).
+        const bool strip_ok = u8ok && prof < strip::kProfileCount && u8_aligned8(im.v) && next[i].padded &&
+                              (im.padded || ((long long)im.v.w * im.v.cn) % 8 == 0);
         if (strip_ok && strip_halo(prof, im.v.cn, true) <= 8 && (op == 2 || op == 3) && it == 1) {
           mode[i] = 2;
           Launch *l = class_of(ls, kOpMorphStrip, k8U, im.v.cn, kh, op == 3, true, prof);
-          BImg b = bimg(im.v, next[i].v);
-          b.pad = (im.padded ? 1 : 0) | (next[i].padded ? 2 : 0);
-          add_img(l, b, im.input);
+          add_img(l, bimg(im.v, next[i].v), im.input);
           u8_bytes(*l, im.v, next[i].v, 1);
           continue;
         }
@@ -532,7 +533,6 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
           const Buf &im = src[i];
           const DImg from = p == 0 ? im.v : tmp[i][(p - 1) % 2].v;
           const DImg dst = p + 1 == np ? next[i].v : tmp[i][p % 2].v;
-          const bool from_pad = p == 0 ? im.padded : true;
           Launch *l;
           if (mode[i] == 1) {
             l = class_of(pl, kOpMorphStrip, k8U, im.v.cn, kh, passes[p], false, prof);
@@ -542,9 +542,7 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
             l = class_of(pl, kOpMorph, k8U, im.v.cn, kh, passes[p]);
             fast::morph_fast_args(mask, kw, kh, im.v.cn, im.v.w, l->ma);
           }
-          BImg b = bimg(from, dst);
-          b.pad = (from_pad ? 1 : 0) | 2;
-          add_img(l, b, p == 0 ? im.input : -1);
+          add_img(l, bimg(from, dst), p == 0 ? im.input : -1);
           u8_bytes(*l, from, dst, depth_size(im.depth));
         }
         for (Launch &l : pl) {

@@ -32,7 +32,6 @@ struct BImg {
   float cv;             // border value as f32
   int wide;             // source rows allow 8-byte loads
   int lanes;            // row-tiled operations: log2 of the threads per row
-  int pad;              // warp strips: bit 0 source, bit 1 destination rows padded to 8-sample words
 };
 
 struct TileQ {
@@ -724,12 +723,12 @@ struct NoArgs {
 // on warp strips (strip.cuh).
 template <class P1, class P2, int CN, int RH, bool MAX1, bool FUSED>
 struct OpMorphStrip {
-  static constexpr int kThreads = 128, kMinBlocks = FUSED ? (P1::KH >= 7 ? 4 : 5) : 6;  // 128 / 102 / 85 registers
+  static constexpr int kThreads = 128, kMinBlocks = FUSED && P1::KH >= 7 ? 4 : 6;  // <= 128 / 85 registers
   static constexpr bool kWarpTiles = true;
   using Args = NoArgs;
   static size_t smem(const Args &) { return 0; }
   static __device__ __forceinline__ void tile(const BImg &im, const Args &, int tx, int ty, int lane) {
-    strip::MorphStrip<P1, P2, CN, RH, MAX1, FUSED>::run(im.s, im.d, im.pad, tx, ty, lane);
+    strip::MorphStrip<P1, P2, CN, RH, MAX1, FUSED>::run(im.s, im.d, tx, ty, lane);
   }
 };
 

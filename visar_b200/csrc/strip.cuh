@@ -2,7 +2,8 @@
 // samples across RH output rows and walks down it, keeping the vertical
 // window in registers; horizontal neighbours come from the adjacent lanes by
 // warp shuffles. The outer lanes of a strip are halo (loaded, not written).
-// No shared memory and no block barriers: each warp streams its own rows.
+// No block barriers: each warp streams its own rows through its own slots of
+// shared memory.
 //
 // Two operations:
 //  * gauss_strip: u8 Gaussian whose fixed-point taps are g * binomial(K)
@@ -35,70 +36,8 @@ namespace strip {
 constexpr unsigned kFull = 0xFFFFFFFFu;
 constexpr int kSPL = 8;  // samples per lane (one 8-byte word)
 
-// Column description of one lane's 8 samples. Lanes whose samples are all
-// inside the row load them with one 8-byte load; lanes entirely outside the
-// stencil's reach (REACH samples beyond the row) load nothing; the few lanes
-// that straddle an edge read each sample through an index precomputed once
-// per tile into shared memory: the border map for Gaussian rows (constant
-// border: the fill value), the fill value (identity) for morphology.
-struct Cols {
-  long long gs;  // first sample of the lane
-  long long n;   // samples per row
-  bool inside;   // all samples inside the row
-  bool edge;     // straddles an edge within reach: indexed loads
-  int *idx;      // this lane's 8 sample indices (-1: fill) when edge
-};
-
-// Per-warp index slots for edge lanes: 8 ints per lane, kWarpsPerBlock warps.
+// Warps per block of the strip kernels (per-warp shared-memory slots).
 constexpr int kWarpsPerBlock = 4;
-
-template <int CN, int REACH>
-__device__ __forceinline__ Cols make_cols(long long gs, long long n, int W, int border, bool ident, int lane) {
-  __shared__ int s_idx[kWarpsPerBlock][32][kSPL];
-  Cols c;
-  c.gs = gs;
-  c.n = n;
-  c.inside = gs >= 0 && gs + kSPL <= n;
-  c.edge = !c.inside && gs + kSPL > -REACH && gs < n + REACH;
-  c.idx = s_idx[(threadIdx.x >> 5) % kWarpsPerBlock][lane];
-  if (c.edge) {
-    for (int k = 0; k < kSPL; k++) {
-      const long long g = gs + k;
-      int m;
-      if (g >= 0 && g < n) {
-        m = (int)g;
-      } else if (ident) {
-        m = -1;
-      } else {
-        const long long px = g >= 0 ? g / CN : -((-g + CN - 1) / CN);
-        const int mx = border_map(px, W, border);
-        m = mx < 0 ? -1 : (int)(mx * CN + (g - px * CN));
-      }
-      c.idx[k] = m;
-    }
-  }
-  __syncwarp();
-  return c;
-}
-
-static __device__ __noinline__ uint2 load8_edge(const uint8_t *row, const int *idx, uint32_t fill) {
-  uint32_t v[2] = {0, 0};
-#pragma unroll
-  for (int k = 0; k < kSPL; k++) {
-    const int m = idx[k];
-    const uint32_t b = m < 0 ? (fill & 0xFFu) : (uint32_t)__ldg(row + m);
-    v[k >> 2] |= b << (8 * (k & 3));
-  }
-  return make_uint2(v[0], v[1]);
-}
-
-__device__ __forceinline__ void store8(uint8_t *row, long long gs, long long n, uint32_t lo, uint32_t hi) {
-  if (gs + kSPL <= n) {
-    *reinterpret_cast<uint2 *>(row + gs) = make_uint2(lo, hi);
-  } else {
-    for (int k = 0; k < kSPL && gs + k < n; k++) row[gs + k] = (uint8_t)((k < 4 ? lo : hi) >> (8 * (k & 3)));
-  }
-}
 
 // The four sample pairs (16-bit lanes) of 8 bytes: pairs (0,1) (2,3) (4,5) (6,7).
 __device__ __forceinline__ void unpack_pairs(uint2 v, uint32_t (&p)[4]) {
@@ -171,8 +110,8 @@ struct GaussGeom {
 // Row queue in shared memory. Each lane copies its 8 samples of source row
 // j + kQD into slot (j + kQD) % kQD with cp.async while row j is computed, so
 // kQD rows per lane are in flight without a register queue to rotate. Lanes
-// that straddle an edge (gathers) or lie outside the row (fill) store their
-// bytes into the slot directly. Slots are lane-private: no barriers.
+// outside the row store the fill into the slot directly. Slots are
+// lane-private: no barriers.
 constexpr int kQD = 8;
 
 __device__ __forceinline__ void cp_async8(uint32_t saddr, const void *g) {
@@ -202,17 +141,8 @@ __device__ __forceinline__ RowQueue row_queue(int lane) {
   return RowQueue{(uint32_t)__cvta_generic_to_shared(&s_q[(threadIdx.x >> 5) % kWarpsPerBlock][0][lane])};
 }
 
-// Starts filling a slot with this lane's 8 samples of `row` (nullptr: the
-// fill value everywhere).
-__device__ __forceinline__ void fetch8(uint32_t saddr, const uint8_t *row, const Cols &c, uint32_t fill) {
-  if (row != nullptr && c.inside) cp_async8(saddr, row + c.gs);
-  else if (row != nullptr && c.edge) st_shared8(saddr, load8_edge(row, c.idx, fill));
-  else st_shared8(saddr, make_uint2(fill, fill));
-}
-
-// Interior tiles (every lane's samples inside the row): a predicated copy of
-// the lane's 8 samples at g, or the fill stored into the slot when !p (g is
-// then not read). No branches.
+// A predicated copy of the lane's 8 samples at g, or the fill stored into
+// the slot when !p (g is then not read). No branches.
 __device__ __forceinline__ void fetch8_inside(uint32_t saddr, const uint8_t *g, bool p, uint32_t fill) {
   asm volatile(
       "{\n .reg .pred q;\n setp.ne.b32 q, %2, 0;\n"
@@ -626,19 +556,6 @@ __device__ __forceinline__ void band_apply(const uint32_t (&h)[PR::KH][4], uint3
     for (int p = 0; p < 4; p++) out[p] = pop3<MAX>(out[p], h[(ROT + AY - a) % KH][p], h[(ROT + AY + a) % KH][p]);
 }
 
-// Pair lanes of samples outside the row set to the identity.
-__device__ __forceinline__ void mask_pairs(uint32_t (&v)[4], const Cols &c, uint32_t ident) {
-  if (c.inside) return;
-#pragma unroll
-  for (int k = 0; k < kSPL; k++) {
-    const long long g = c.gs + k;
-    if (g < 0 || g >= c.n) {
-      const uint32_t m = (k & 1) ? 0xFFFF0000u : 0x0000FFFFu;
-      v[k >> 1] = (v[k >> 1] & ~m) | (ident & m);
-    }
-  }
-}
-
 // One pass (FUSED = false: extremum MAX1 with element P1) or two fused
 // passes (MAX1 with P1, then !MAX1 with P2, which has P1's height) over a
 // strip whose outer HALO lanes are not written. A lane's first-pass value at
@@ -661,16 +578,16 @@ struct MorphStrip {
   static constexpr uint32_t I1 = MAX1 ? 0u : 0xFFFFFFFFu;
   static constexpr uint32_t I1p = MAX1 ? 0u : 0x00FF00FFu;
   static constexpr uint32_t I2p = MAX2 ? 0u : 0x00FF00FFu;
-  // Tile modes: every lane inside the row; lanes inside, entirely outside
-  // (predicated fills) or straddling the row's end with an 8-byte copy into
-  // the row padding (masked per pair); any other tile (per-sample paths).
-  enum Mode { kInside, kEdge, kSlow };
+  // Tile modes: every lane inside the row; or lanes inside, entirely
+  // outside (predicated fills) or straddling the row's end with an 8-byte
+  // copy into the row padding (masked per pair: the plan hands the strips
+  // rows readable and writable up to their length rounded up to 8 samples).
+  enum Mode { kInside, kEdge };
 
   const DImg s, d;  // copies (kept in registers across the row loop)
   long long n, gs;
   int H, first, nsrc, ylim;
-  bool out_lane, live;
-  Cols c;
+  bool out_lane, live, inside;
   RowQueue q;
   // kInside / kEdge: the next source row to fetch and the next output row,
   // as running pointers at this lane's samples (advanced by a stride per
@@ -685,7 +602,7 @@ struct MorphStrip {
   __device__ __forceinline__ MorphStrip(const DImg &s_, const DImg &d_, int tx, int ty, int lane) : s(s_), d(d_) {
     n = (long long)s.w * CN;
     gs = ((long long)tx * OL - HALO + lane) * kSPL;
-    c = make_cols<CN, (M1 + M2) * CN>(gs, n, s.w, 0, true, lane);
+    inside = gs >= 0 && gs + kSPL <= n;
     H = s.h;
     const int y0 = ty * RH;
     first = y0 - AY2 - AY1;
@@ -703,32 +620,21 @@ struct MorphStrip {
     op = d.p + (long long)y0 * d.stride + gs;
   }
 
-  // Source row j into its slot (rows j >= nsrc: nothing is read). kInside and
-  // kEdge fetch rows in order, one per call.
+  // Source row j into its slot (rows outside [jlo, jhi): the fill). Rows
+  // are fetched in order, one per call.
   template <int MODE>
   __device__ __forceinline__ void fetch(int j) {
-    if constexpr (MODE != kSlow) {
-      fetch8_inside(q.slot(j), fp, (unsigned)(j - jlo) < (unsigned)(jhi - jlo), I1);
-      fp += s.stride;
-    } else {
-      const int sy = first + j;
-      const bool in = sy >= 0 && sy < H;
-      if (j < nsrc) fetch8(q.slot(j), in ? row_ptr<const uint8_t>(s, sy) : nullptr, c, I1);
-    }
+    fetch8_inside(q.slot(j), fp, (unsigned)(j - jlo) < (unsigned)(jhi - jlo), I1);
+    fp += s.stride;
   }
 
-  // Output row y, written when it belongs to the tile and the image. kInside
-  // and kEdge put rows y0, y0 + 1, ... in order, one per call.
+  // The next output row (rows y0, y0 + 1, ... in order, one per call),
+  // written when it belongs to the tile and the image.
   template <int MODE>
-  __device__ __forceinline__ void put(int y, const uint32_t (&o)[4]) {
-    const uint2 o8 = pack_pairs(o);
-    if constexpr (MODE != kSlow) {
-      st_global8_if(op, o8, out_lane && yout < ylim);
-      op += d.stride;
-      yout++;
-    } else {
-      if (out_lane && y < ylim) store8(row_ptr<uint8_t>(d, y), gs, n, o8.x, o8.y);
-    }
+  __device__ __forceinline__ void put(const uint32_t (&o)[4]) {
+    st_global8_if(op, pack_pairs(o), out_lane && yout < ylim);
+    op += d.stride;
+    yout++;
   }
 
   // Source row j; PH = j mod KH1. Rows past nsrc (the last group of KH1)
@@ -750,7 +656,7 @@ struct MorphStrip {
     band_apply<P1, CN, MAX1, (PH + 1) % KH1>(h1, o1);
     const int y1 = first + j - (KH1 - 1) + AY1;  // first-pass row completed
     if constexpr (!FUSED) {
-      put<MODE>(y1, o1);
+      put<MODE>(o1);
     } else {
       // First-pass row t2 = j - (KH1 - 1) goes to slot t2 mod KH2; values
       // outside the image are the second pass's identity.
@@ -761,11 +667,10 @@ struct MorphStrip {
         const uint32_t v = rin ? o1[p] : I2p;
         h2[S2][p] = MODE == kEdge ? (v & keep[p]) | (I2p & ~keep[p]) : v;
       }
-      if constexpr (MODE == kSlow) mask_pairs(h2[S2], c, I2p);
       if (WARM && j < (KH1 - 1) + (KH2 - 1)) return;
       uint32_t o2[4];
       band_apply<P2, CN, MAX2, (PH + 2) % KH2>(h2, o2);
-      put<MODE>(y1 - (KH2 - 1) + AY2, o2);
+      put<MODE>(o2);
     }
   }
 
@@ -792,14 +697,10 @@ struct MorphStrip {
     for (int j = 0; j < nsrc; j += KH1) steps<MODE, true>(j, std::make_integer_sequence<int, KH1>{});
   }
 
-  // pad: bit 0 = source rows readable, bit 1 = destination rows writable, up
-  // to their length rounded up to 8 samples (the engine's pitched images).
-  static __device__ __forceinline__ void run(const DImg &s, const DImg &d, int pad, int tx, int ty, int lane) {
+  static __device__ __forceinline__ void run(const DImg &s, const DImg &d, int tx, int ty, int lane) {
     MorphStrip m(s, d, tx, ty, lane);
-    const bool straddle = m.live && !m.c.inside;
-    if (__all_sync(kFull, m.c.inside)) m.template rows<kInside>();
-    else if (__all_sync(kFull, !straddle || (pad & 3) == 3)) m.template rows<kEdge>();
-    else m.template rows<kSlow>();
+    if (__all_sync(kFull, m.inside)) m.template rows<kInside>();
+    else m.template rows<kEdge>();
   }
 };
 
