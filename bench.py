@@ -19,7 +19,7 @@ Gpix/s counts input pixels (width x height) once per image per step.
 
   value : inputs resident in HBM; CUDA events on the launching stream. The
           batched inputs (1.2 GB) are larger than L2; plain-1080p flushes L2
-          (256 MiB write) before every timed step.
+          (256 MiB write, then a 256 MiB read) before every timed step.
   e2e   : the same work through the public API from pinned host buffers:
           host->device copy of every input and device->host copy of every
           result inside each timed step.
@@ -207,6 +207,20 @@ class Ctx:
             self.dist.destroy_process_group()
 
 
+class L2Flush:
+    """Evicts L2 (126 MB) before a timed step: a 256 MiB write, then a 256 MiB
+    read of another buffer, so that the step starts on clean lines instead of
+    writing back the flush's own dirty ones inside its timed region."""
+
+    def __init__(self, torch):
+        self.w = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+        self.r = torch.zeros(64 << 20, dtype=torch.int32, device="cuda")
+
+    def __call__(self, i):
+        self.w.fill_(i & 0xFF)
+        self.r.max()
+
+
 # ----------------------------------------------------------- batched-mixed
 
 N_IMAGES = 256
@@ -335,6 +349,9 @@ def bench_batched(args, ctx):
 
     tuned = tune_workload(args, ctx, "batched-mixed", [(h, w, c, np.uint8) for (h, w, c) in shapes], c2_stages(B),
                           fill)
+    if args.rows:  # the full plan's strip tile height on a reduced plan (profiler captures)
+        for key in ("gauss_strip.u8.c1.k5.rows", "morph_strip.u8.c1.k5.ell5.open.rows"):
+            B.tune_set(key, args.rows)
     plan = B.Batch([(h, w, c, np.uint8) for (h, w, c) in shapes], c2_stages(B))
     fill(plan)
     del bases
@@ -1061,7 +1078,7 @@ def bench_plain(args, ctx):
     d_img = torch.from_numpy(img).cuda()
     d_f = torch.from_numpy(f).cuda()
     d_outs = alloc_outs(torch)
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    flush = L2Flush(torch)
     vb.set_async(True)
     for _ in range(args.warmup):
         run_step(vb, d_img, d_f, maff, mper, d_outs)
@@ -1069,7 +1086,7 @@ def bench_plain(args, ctx):
     n0 = vb.launch_count()
     with Clocks(ctx.dev) as clk:
         ms = ctx.timed(lambda: run_step(vb, d_img, d_f, maff, mper, d_outs), args.steps,
-                       before=lambda i: flush.fill_(i & 0xFF))
+                       before=flush)
     launches = vb.launch_count() - n0
     ctx.barrier()
     ms_step = ctx.max_over_ranks(ms) / args.steps
@@ -1082,7 +1099,7 @@ def bench_plain(args, ctx):
             op_call(vb, name, d_img, d_f, maff, mper, d_outs)
         n = max(5, args.steps // 2)
         per_op[name] = ctx.timed(lambda: op_call(vb, name, d_img, d_f, maff, mper, d_outs), n,
-                                 before=lambda i: flush.fill_(i & 0xFF)) / n
+                                 before=flush) / n
     vb.set_async(False)
     dom = max(per_op, key=lambda k: per_op[k])
     peak, peak_kind = load_peaks()
@@ -1097,7 +1114,7 @@ def bench_plain(args, ctx):
         run_step(vb, h_img, h_f, maff, mper, h_outs)
     ctx.barrier()
     e_ms = ctx.max_over_ranks(ctx.timed(lambda: run_step(vb, h_img, h_f, maff, mper, h_outs), args.steps,
-                                        before=lambda i: flush.fill_(i & 0xFF))) / args.steps
+                                        before=flush)) / args.steps
     e2e = PIX_PER_STEP * ctx.world / (e_ms / 1e3) / 1e9
     ctx.barrier()
     cpu, parity = None, None
@@ -1120,7 +1137,7 @@ def bench_plain(args, ctx):
         "scaling": "weak", "vs_baseline": None, "dtype": "u8+f32", "data": "synthetic",
         "config": {"workload": "plain-1080p", "frame": f"{W}x{H}x3 u8 + {W}x{H}x1 f32",
                    "ops": [o[0] for o in OPS], "pixels_per_step": PIX_PER_STEP,
-                   "l2": "flushed before every timed step (256 MiB write)", "parallelism": f"replicas{ctx.world}",
+                   "l2": "flushed before every timed step (256 MiB write, then a 256 MiB read)", "parallelism": f"replicas{ctx.world}",
                    "per_op_ms": per_op},
         "e2e": {"value": e2e, "unit": "Gpix/s", "h2d_bytes_per_step": H2D_BYTES, "d2h_bytes_per_step": D2H_BYTES,
                 "ms_per_step": e_ms},
@@ -1191,7 +1208,7 @@ def bench_c0(args, ctx):
     x = c0_input()
     d_x = torch.from_numpy(x).cuda()
     d_outs = [torch.empty((C0_H, C0_W), dtype=torch.uint8, device="cuda") for _ in range(5)]
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    flush = L2Flush(torch)
     vb.set_async(True)
     steps = max(args.steps, 50)
     for _ in range(args.warmup):
@@ -1199,7 +1216,7 @@ def bench_c0(args, ctx):
     ctx.barrier()
     n0 = vb.launch_count()
     with Clocks(ctx.dev) as clk:
-        ms = ctx.timed(lambda: c0_pipeline(vb, d_x, d_outs), steps, before=lambda i: flush.fill_(i & 0xFF))
+        ms = ctx.timed(lambda: c0_pipeline(vb, d_x, d_outs), steps, before=flush)
     launches = vb.launch_count() - n0
     ctx.barrier()
     ms_step = ctx.max_over_ranks(ms) / steps
@@ -1213,7 +1230,7 @@ def bench_c0(args, ctx):
     plan.input(0).copy_(d_x)
     for _ in range(args.warmup):
         plan.run_graph()
-    g_ms = ctx.max_over_ranks(ctx.timed(plan.run_graph, steps, before=lambda i: flush.fill_(i & 0xFF))) / steps
+    g_ms = ctx.max_over_ranks(ctx.timed(plan.run_graph, steps, before=flush)) / steps
     vb.set_async(False)
     # e2e: host images in pinned memory through the per-call C ABI.
     h_x = torch.empty(x.shape, dtype=torch.uint8, pin_memory=True).numpy()
@@ -1245,7 +1262,7 @@ def bench_c0(args, ctx):
         "vs_baseline": None, "dtype": "u8", "data": "synthetic",
         "config": {"workload": "c0-640x480", "image": f"{C0_W}x{C0_H}x3 u8, seed 0, 8 rectangles", "stages": C0_NAMES,
                    "latency_us": ms_step * 1e3, "graph_us": g_ms * 1e3, "graph_gpix_s": px / (g_ms / 1e3) / 1e9,
-                   "alg_bytes_per_step": C0_BYTES, "l2": "flushed before every timed step (256 MiB write)"},
+                   "alg_bytes_per_step": C0_BYTES, "l2": "flushed before every timed step (256 MiB write, then a 256 MiB read)"},
         "e2e": {"value": px * ctx.world / (e_ms / 1e3) / 1e9, "unit": "Gpix/s", "h2d_bytes_per_step": C0_BYTES // 2,
                 "d2h_bytes_per_step": 5 * px, "ms_per_step": e_ms},
         "cpu_baseline": cpu,
@@ -1284,10 +1301,10 @@ N_W, N_H = 3840, 2160
 
 
 def timed_op(ctx, fn, n, flush):
-    """Mean ms of fn over n launches, L2 flushed (256 MiB write) before each."""
+    """Mean ms of fn over n launches, L2 flushed (256 MiB write, then a 256 MiB read) before each."""
     for _ in range(3):
         fn()
-    return ctx.timed(fn, n, before=lambda i: flush.fill_(i & 0xFF)) / n
+    return ctx.timed(fn, n, before=flush) / n
 
 
 def bench_next(args, ctx):
@@ -1300,7 +1317,7 @@ def bench_next(args, ctx):
     from oracle import oracle as O
     synth = load_synth()
     peak, peak_kind = load_peaks()
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    flush = L2Flush(torch)
     n = max(10, args.steps)
     cpu_ok = ctx.rank == 0 and ctx.world == 1 and not args.no_cpu_baseline
     out = {}
@@ -1373,7 +1390,7 @@ def bench_next(args, ctx):
     torch.cuda.synchronize()
     vb.set_async(False)
     return {"workload": "next-rows", "peak_gbs": peak, "peak_kind": peak_kind,
-            "timing": "device images, CUDA events, L2 flushed (256 MiB write) before each launch",
+            "timing": "device images, CUDA events, L2 flushed (256 MiB write, then a 256 MiB read) before each launch",
             "alg_bytes": "source + destination bytes once (remap adds its two f32 maps)", "calls": out}
 
 
@@ -1410,6 +1427,8 @@ def main():
     ap.add_argument("--duration", type=float, default=20.0, help="seconds per arrival rate (served workload)")
     ap.add_argument("--images", type=int, default=0,
                     help="batched-mixed: the first N images only (a reduced plan for profiler captures; not a bench line)")
+    ap.add_argument("--rows", type=int, default=0, choices=[0, 8, 32, 64],
+                    help="batched-mixed: strip tile height (with --images: the full plan's 64 on a reduced plan)")
     ap.add_argument("--frames", type=int, default=0,
                     help="video-4k: N frames in HBM instead of 300 (a reduced case for profiler captures; not a bench line)")
     args = ap.parse_args()

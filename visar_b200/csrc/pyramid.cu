@@ -58,11 +58,13 @@ constexpr int kDownElems = 256;   // output elements (pixels x channels) per til
 constexpr int kThreads = 256;
 
 // pyrDown tile: output rows [oy0, oy0 + kDownRows), output pixels [ox0, ox0 + twp).
-template <class T>
+// CN_: the channel count when compiled in (1, 3, 4), else 0 (cn at run time).
+template <class T, int CN_>
 __global__ void __launch_bounds__(kThreads) k_pyr_down(const uint8_t *__restrict__ src, long long sstride, int sw, int sh,
                                                        uint8_t *__restrict__ dst, long long dstride, int dw, int dh,
-                                                       int cn, int twp, int border) {
+                                                       int cn_rt, int twp, int border) {
   using A = typename PyrAcc<T>::A;
+  const int cn = CN_ > 0 ? CN_ : cn_rt;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   A *V = reinterpret_cast<A *>(smem_raw);
   const int ox0 = blockIdx.x * twp;
@@ -71,37 +73,39 @@ __global__ void __launch_bounds__(kThreads) k_pyr_down(const uint8_t *__restrict
   const int nrows = min(kDownRows, dh - oy0);
   const int spx = 2 * npx + 3;  // source pixels 2*ox0-2 .. 2*(ox0+npx-1)+2
   const int span = spx * cn;
-  // Phase 1: vertical sums, V[r * span + e].
+  // The tile's 2 * nrows + 3 source rows, border-mapped once.
+  constexpr int NS = 2 * kDownRows + 3;
+  __shared__ const uint8_t *s_row[NS];
+  if (threadIdx.x < NS) s_row[threadIdx.x] = src + (long long)border_map(2 * oy0 - 2 + (int)threadIdx.x, sh, border) * sstride;
+  __syncthreads();
+  // Columns need the border map only in a row's first and last tiles.
+  const bool inner = 2 * ox0 - 2 >= 0 && 2 * (ox0 + npx - 1) + 2 < sw;
+  const int e0 = (2 * ox0 - 2) * cn;
+  // Phase 1: vertical sums, V[r * span + e]; every row of a column is loaded
+  // before the sums, so the loads are in flight together.
   for (int e = threadIdx.x; e < span; e += kThreads) {
-    const int px = 2 * ox0 - 2 + e / cn;
-    const int ch = e - (e / cn) * cn;
-    const int mx = border_map(px, sw, border);
-    const int se = mx * cn + ch;
-    int ys[5];
-    for (int j = 0; j < 4; j++) ys[j] = border_map(2 * oy0 - 2 + j, sh, border);
-    A r0 = ld<T>(src, sstride, ys[0], se), r1 = ld<T>(src, sstride, ys[1], se);
-    A r2 = ld<T>(src, sstride, ys[2], se), r3 = ld<T>(src, sstride, ys[3], se);
-    for (int r = 0; r < nrows; r++) {
-      const int yb = 2 * (oy0 + r) - 2;
-      const A r4 = ld<T>(src, sstride, border_map(yb + 4, sh, border), se);
-      V[r * span + e] = tap5(r0, r1, r2, r3, r4);
-      const A r5 = r + 1 < nrows ? ld<T>(src, sstride, border_map(yb + 5, sh, border), se) : r4;
-      r0 = r2;
-      r1 = r3;
-      r2 = r4;
-      r3 = r5;
+    int se = e0 + e;
+    if (!inner) {
+      const int px = 2 * ox0 - 2 + e / cn;
+      se = border_map(px, sw, border) * cn + (e - (e / cn) * cn);
     }
+    A r[NS];
+#pragma unroll
+    for (int k = 0; k < NS; k++) r[k] = k < 2 * nrows + 3 ? (A) reinterpret_cast<const T *>(s_row[k])[se] : (A)0;
+#pragma unroll
+    for (int rr = 0; rr < kDownRows; rr++)
+      if (rr < nrows) V[rr * span + e] = tap5(r[2 * rr], r[2 * rr + 1], r[2 * rr + 2], r[2 * rr + 3], r[2 * rr + 4]);
   }
   __syncthreads();
   // Phase 2: output element j of the tile row sits over padded element 2j - j % cn + 2cn.
   const int ne = npx * cn;
-  for (int idx = threadIdx.x; idx < nrows * ne; idx += kThreads) {
-    const int r = idx / ne;
-    const int j = idx - r * ne;
-    const int c = 2 * j - j % cn + 2 * cn;
-    const A *v = V + r * span + c;
-    const A s = tap5(v[-2 * cn], v[-cn], v[0], v[cn], v[2 * cn]);
-    reinterpret_cast<T *>(dst + (long long)(oy0 + r) * dstride)[(long long)ox0 * cn + j] = pyr_finish<T, 8>(s);
+  for (int r = 0; r < nrows; r++) {
+    T *orow = reinterpret_cast<T *>(dst + (long long)(oy0 + r) * dstride) + (long long)ox0 * cn;
+    for (int j = threadIdx.x; j < ne; j += kThreads) {
+      const int c = 2 * j - j % cn + 2 * cn;
+      const A *v = V + r * span + c;
+      orow[j] = pyr_finish<T, 8>(tap5(v[-2 * cn], v[-cn], v[0], v[cn], v[2 * cn]));
+    }
   }
 }
 
@@ -131,10 +135,11 @@ constexpr int kUpRows = 8;  // source rows per tile (16 output rows)
 __device__ __forceinline__ int up_row(int y, int h) { return y < 0 ? (h > 1 ? 1 : 0) : y >= h ? h - 1 : y; }
 
 // pyrUp tile: source rows [sy0, sy0 + kUpRows), source pixels [sx0, sx0 + twp).
-template <class T>
+template <class T, int CN_>
 __global__ void __launch_bounds__(kThreads) k_pyr_up(const uint8_t *__restrict__ src, long long sstride, int sw, int sh,
-                                                     uint8_t *__restrict__ dst, long long dstride, int cn, int twp) {
+                                                     uint8_t *__restrict__ dst, long long dstride, int cn_rt, int twp) {
   using A = typename PyrAcc<T>::A;
+  const int cn = CN_ > 0 ? CN_ : cn_rt;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int sx0 = blockIdx.x * twp;
   const int sy0 = blockIdx.y * kUpRows;
@@ -143,32 +148,43 @@ __global__ void __launch_bounds__(kThreads) k_pyr_up(const uint8_t *__restrict__
   const int span = (npx + 2) * cn;  // source pixels sx0-1 .. sx0+npx
   A *E = reinterpret_cast<A *>(smem_raw);
   A *O = E + kUpRows * span;
+  // The tile's nrows + 2 source rows, mapped once.
+  constexpr int NS = kUpRows + 2;
+  __shared__ const uint8_t *s_row[NS];
+  if (threadIdx.x < NS) s_row[threadIdx.x] = src + (long long)up_row(sy0 - 1 + (int)threadIdx.x, sh) * sstride;
+  __syncthreads();
+  const bool inner = sx0 - 1 >= 0 && sx0 + npx < sw;
+  // Every row of a column is loaded before the sums (loads in flight together).
   for (int e = threadIdx.x; e < span; e += kThreads) {
-    const int px = sx0 - 1 + e / cn;
-    const int ch = e - (e / cn) * cn;
-    const int mx = px < 0 ? (sw > 1 ? 1 : 0) : px >= sw ? sw - 1 : px;
-    const int se = mx * cn + ch;
-    A a = ld<T>(src, sstride, up_row(sy0 - 1, sh), se);
-    A b = ld<T>(src, sstride, sy0, se);
-    for (int r = 0; r < nrows; r++) {
-      const A c = ld<T>(src, sstride, up_row(sy0 + r + 1, sh), se);
-      E[r * span + e] = up_even(a, b, c);
-      O[r * span + e] = up_odd(b, c);
-      a = b;
-      b = c;
+    int se = (sx0 - 1) * cn + e;
+    if (!inner) {
+      const int px = sx0 - 1 + e / cn;
+      const int mx = px < 0 ? (sw > 1 ? 1 : 0) : px >= sw ? sw - 1 : px;
+      se = mx * cn + (e - (e / cn) * cn);
+    }
+    A r[NS];
+#pragma unroll
+    for (int k = 0; k < NS; k++) r[k] = k < nrows + 2 ? (A) reinterpret_cast<const T *>(s_row[k])[se] : (A)0;
+#pragma unroll
+    for (int rr = 0; rr < kUpRows; rr++) {
+      if (rr < nrows) {
+        E[rr * span + e] = up_even(r[rr], r[rr + 1], r[rr + 2]);
+        O[rr * span + e] = up_odd(r[rr + 1], r[rr + 2]);
+      }
     }
   }
   __syncthreads();
   // Output pixel 2p (+1) of tile row r; q[p] is smem element (p - sx0 + 1) * cn.
   const int ne = 2 * npx * cn;
-  for (int idx = threadIdx.x; idx < 2 * nrows * ne; idx += kThreads) {
-    const int rr = idx / ne;  // output row within the tile
-    const int j = idx - rr * ne;
-    const int opx = j / cn, ch = j - opx * cn;
-    const int p = opx >> 1;
-    const A *q = ((rr & 1) ? O : E) + (rr >> 1) * span + (p + 1) * cn + ch;
-    const A s = (opx & 1) ? up_odd(q[0], q[cn]) : up_even(q[-cn], q[0], q[cn]);
-    reinterpret_cast<T *>(dst + (long long)(2 * sy0 + rr) * dstride)[(long long)2 * sx0 * cn + j] = pyr_finish<T, 6>(s);
+  for (int rr = 0; rr < 2 * nrows; rr++) {  // output row within the tile
+    T *orow = reinterpret_cast<T *>(dst + (long long)(2 * sy0 + rr) * dstride) + (long long)2 * sx0 * cn;
+    const A *qrow = ((rr & 1) ? O : E) + (rr >> 1) * span;
+    for (int j = threadIdx.x; j < ne; j += kThreads) {
+      const int opx = j / cn, ch = j - opx * cn;
+      const A *q = qrow + ((opx >> 1) + 1) * cn + ch;
+      const A s = (opx & 1) ? up_odd(q[0], q[cn]) : up_even(q[-cn], q[0], q[cn]);
+      orow[j] = pyr_finish<T, 6>(s);
+    }
   }
 }
 
@@ -208,7 +224,12 @@ cudaError_t pyr_down_t(const DImg &s, const DImg &d, int border, cudaStream_t st
   const int twp = std::max(1, kDownElems / s.cn);
   const size_t smem = (size_t)kDownRows * (2 * twp + 3) * s.cn * sizeof(A);
   dim3 grid((d.w + twp - 1) / twp, (d.h + kDownRows - 1) / kDownRows);
-  k_pyr_down<T><<<grid, kThreads, smem, st>>>(s.p, s.stride, s.w, s.h, d.p, d.stride, d.w, d.h, s.cn, twp, border);
+  switch (s.cn) {
+    case 1: k_pyr_down<T, 1><<<grid, kThreads, smem, st>>>(s.p, s.stride, s.w, s.h, d.p, d.stride, d.w, d.h, 1, twp, border); break;
+    case 3: k_pyr_down<T, 3><<<grid, kThreads, smem, st>>>(s.p, s.stride, s.w, s.h, d.p, d.stride, d.w, d.h, 3, twp, border); break;
+    case 4: k_pyr_down<T, 4><<<grid, kThreads, smem, st>>>(s.p, s.stride, s.w, s.h, d.p, d.stride, d.w, d.h, 4, twp, border); break;
+    default: k_pyr_down<T, 0><<<grid, kThreads, smem, st>>>(s.p, s.stride, s.w, s.h, d.p, d.stride, d.w, d.h, s.cn, twp, border);
+  }
   return cudaGetLastError();
 }
 
@@ -225,7 +246,12 @@ cudaError_t pyr_up_t(const DImg &s, const DImg &d, cudaStream_t st) {
   const int twp = std::max(1, 128 / s.cn);
   const size_t smem = (size_t)2 * kUpRows * (twp + 2) * s.cn * sizeof(A);
   dim3 grid((s.w + twp - 1) / twp, (s.h + kUpRows - 1) / kUpRows);
-  k_pyr_up<T><<<grid, kThreads, smem, st>>>(s.p, s.stride, s.w, s.h, d.p, d.stride, s.cn, twp);
+  switch (s.cn) {
+    case 1: k_pyr_up<T, 1><<<grid, kThreads, smem, st>>>(s.p, s.stride, s.w, s.h, d.p, d.stride, 1, twp); break;
+    case 3: k_pyr_up<T, 3><<<grid, kThreads, smem, st>>>(s.p, s.stride, s.w, s.h, d.p, d.stride, 3, twp); break;
+    case 4: k_pyr_up<T, 4><<<grid, kThreads, smem, st>>>(s.p, s.stride, s.w, s.h, d.p, d.stride, 4, twp); break;
+    default: k_pyr_up<T, 0><<<grid, kThreads, smem, st>>>(s.p, s.stride, s.w, s.h, d.p, d.stride, s.cn, twp);
+  }
   return cudaGetLastError();
 }
 
