@@ -1427,7 +1427,7 @@ def main():
     ap.add_argument("--duration", type=float, default=20.0, help="seconds per arrival rate (served workload)")
     ap.add_argument("--images", type=int, default=0,
                     help="batched-mixed: the first N images only (a reduced plan for profiler captures; not a bench line)")
-    ap.add_argument("--rows", type=int, default=0, choices=[0, 8, 32, 64],
+    ap.add_argument("--rows", type=int, default=0, choices=[0, 8, 32, 64, 128],
                     help="batched-mixed: strip tile height (with --images: the full plan's 64 on a reduced plan)")
     ap.add_argument("--frames", type=int, default=0,
                     help="video-4k: N frames in HBM instead of 300 (a reduced case for profiler captures; not a bench line)")

@@ -38,8 +38,8 @@ from . import batch as B
 
 # Candidate values per field, by op (the first word of a class key).
 CANDIDATES = {
-    "gauss_strip": {"rows": (8, 32, 64), "per_sm": (2, 4, 5)},
-    "morph_strip": {"rows": (8, 32, 64), "per_sm": (2, 3, 4)},
+    "gauss_strip": {"rows": (8, 32, 64, 128), "per_sm": (2, 4, 5)},
+    "morph_strip": {"rows": (8, 32, 64, 128), "per_sm": (2, 3, 4)},
     "gauss": {"rows": (8, 16, 32), "per_sm": (2, 4)},
     "morph": {"per_sm": (2, 4)},
     "gray": {"rows": (1, 2, 4, 8, 16), "vec": (8, 16), "per_sm": (2, 4, 6)},

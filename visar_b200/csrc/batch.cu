@@ -280,11 +280,12 @@ void tune_and_tile(Launch &L, int num_sms) {
       break;
     }
     case kOpGaussStrip: case kOpMorphStrip: {
-      // Warp tiles of 64 (Gaussian, one-channel morphology), 32 or 8 rows:
-      // the tallest that leaves ~8 tiles per resident warp slot (taller
-      // tiles re-read fewer halo rows).
+      // Warp tiles of 128 (one-channel images), 64 (Gaussian, one-channel
+      // morphology), 32 or 8 rows: by default the tallest of 64/32/8 that
+      // leaves ~8 tiles per resident warp slot (taller tiles re-read fewer
+      // halo rows); 128 when tuned.
       const bool has64 = L.op == kOpGaussStrip || L.cn == 1;
-      if (tuned == 8 || tuned == 32 || (tuned == 64 && has64)) {
+      if (tuned == 8 || tuned == 32 || (tuned == 64 && has64) || (tuned == 128 && L.cn == 1)) {
         L.rows = tuned;
         retile();
         break;

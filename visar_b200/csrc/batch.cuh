@@ -875,8 +875,9 @@ cudaError_t launch_morph_strip_rh(const LaunchRun &r, bool max1, bool fused, cud
 template <class PR, int CN>
 cudaError_t launch_morph_strip_prof(const LaunchRun &r, int rows, bool max1, bool fused, cudaStream_t st) {
   if (rows == 8) return launch_morph_strip_rh<PR, CN, 8>(r, max1, fused, st);
-  if constexpr (CN == 1) {  // 64-row tiles: one-channel images only (compile time)
+  if constexpr (CN == 1) {  // 64- and 128-row tiles: one-channel images only (compile time)
     if (rows == 64) return launch_morph_strip_rh<PR, CN, 64>(r, max1, fused, st);
+    if (rows == 128) return launch_morph_strip_rh<PR, CN, 128>(r, max1, fused, st);
   }
   return launch_morph_strip_rh<PR, CN, 32>(r, max1, fused, st);
 }

@@ -9,6 +9,9 @@ template <int K, int CN>
 static cudaError_t gauss_rows(const LaunchRun &r, int rows, int border, cudaStream_t st) {
   const strip::GaussArgs a{border};
   if (rows == 8) return launch_op<OpGaussStrip<K, CN, 8>>(r, a, st);
+  if constexpr (CN == 1) {  // 128-row tiles: one-channel images only (compile time)
+    if (rows == 128) return launch_op<OpGaussStrip<K, CN, 128>>(r, a, st);
+  }
   if (rows == 64) return launch_op<OpGaussStrip<K, CN, 64>>(r, a, st);
   return launch_op<OpGaussStrip<K, CN, 32>>(r, a, st);
 }
