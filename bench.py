@@ -907,6 +907,7 @@ def bench_served(args, ctx):
                 row["fallback_calls"] = st["fallback_calls"]
                 row["deferred"] = st["deferred"]
                 row["solo"] = st["solo"]
+                row["schedule_s"] = st["schedule_s"]
         results.append(row)
     clk.__exit__(None, None, None)
     clocks = clk.summary()

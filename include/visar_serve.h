@@ -33,8 +33,8 @@ enum visar_serve_mode { VISAR_SERVE_BATCHED = 0, VISAR_SERVE_PLAIN = 1 };
 typedef struct visar_server_config {
     size_t pool_bytes;   /* device pool for intermediate and final results (0: 64 GiB) */
     int mode;            /* enum visar_serve_mode */
-    int max_inflight;    /* scheduling rounds queued on the GPU at once (0: 4) */
-    int streams;         /* streams the stage groups of a round spread over (0: 4) */
+    int max_inflight;    /* scheduling rounds queued on the GPU at once (0: 2; fewer rounds in flight make larger groups) */
+    int streams;         /* streams the stage groups of a round spread over (0: 8) */
 } visar_server_config;
 
 typedef struct visar_server visar_server;
@@ -49,6 +49,10 @@ typedef struct visar_server_stats {
     uint64_t deferred;        /* stage groups put off to a later round for pool or staging memory */
     uint64_t solo;            /* requests run whole through the per-call entry points: new, with no
                                  request sharing their first stage (a round would run them alone) */
+    double schedule_s;        /* scheduler thread time spent building and enqueuing rounds, of which: */
+    double build_s;           /*   building stage groups (shapes, classes, tables) */
+    double upload_s;          /*   staging and enqueuing their descriptor and table copies */
+    double launch_s;          /*   enqueuing their launches */
 } visar_server_stats;
 
 int visar_server_create(const visar_server_config *cfg, visar_server **out);

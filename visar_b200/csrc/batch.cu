@@ -8,6 +8,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <tuple>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -400,6 +401,28 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
       if (border < 0 || border > 4) return VISAR_UNSUPPORTED;
       if (kw_in < 0 || kh_in < 0) return VISAR_INVALID_ARGUMENT;
       if (const int rc = repack_unaligned(true); rc != VISAR_OK) return rc;
+      // The taps depend only on the size and the depth class: computed once
+      // per stage (a served round holds hundreds of images of one stage).
+      std::map<int, std::vector<int64_t>> fixed_taps;
+      std::map<int, std::vector<double>> f_taps;
+      auto fixed_of = [&](int kw) -> const std::vector<int64_t> & {
+        auto it = fixed_taps.find(kw);
+        if (it == fixed_taps.end()) {
+          std::vector<int64_t> t(kw);
+          gaussian_kernel_fixed(t.data(), kw, sx, 8);
+          it = fixed_taps.emplace(kw, std::move(t)).first;
+        }
+        return it->second;
+      };
+      auto float_of = [&](int kw) -> const std::vector<double> & {
+        auto it = f_taps.find(kw);
+        if (it == f_taps.end()) {
+          std::vector<double> t(kw);
+          gaussian_kernel(t.data(), kw, sx);
+          it = f_taps.emplace(kw, std::move(t)).first;
+        }
+        return it->second;
+      };
       for (size_t i = 0; i < n; i++) {
         const Buf &im = src[i];
         if (!B.image(im.v.w, im.v.h, im.v.cn, im.depth, next[i])) return VISAR_OUT_OF_MEMORY;
@@ -415,8 +438,7 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
           a.border = border;
           a.symx = a.symy = 1;
           if (u8) {
-            std::vector<int64_t> t(kw);
-            gaussian_kernel_fixed(t.data(), kw, sx, 8);
+            const std::vector<int64_t> &t = fixed_of(kw);
             long long sum = 0;
             for (int j = 0; j < kw; j++) {
               ok = ok && t[j] >= 0 && t[j] == t[kw - 1 - j];
@@ -426,8 +448,7 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
             ok = ok && sum <= 256;
             a.shift = 16;
           } else {
-            std::vector<double> t(kw);
-            gaussian_kernel(t.data(), kw, sx);
+            const std::vector<double> &t = float_of(kw);
             for (int j = 0; j < kw; j++) {
               const float f = (float)t[j];
               ok = ok && f >= 0.0f && f == (float)t[kw - 1 - j];
@@ -440,8 +461,7 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
           continue;
         }
         if (u8) {
-          std::vector<int64_t> t(kw);
-          gaussian_kernel_fixed(t.data(), kw, sx, 8);
+          const std::vector<int64_t> &t = fixed_of(kw);
           // Strips map rows past the bottom edge in closed form (images taller
           // than the radius), take border columns from their own row window
           // (not the far end of the row: no wrap), and read and write whole
@@ -558,6 +578,26 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
       const double fx = st.d[0], fy = st.d[1];
       if (interp < 0 || interp > 4) return VISAR_UNSUPPORTED;
       if (!(fx > 0) || !(fy > 0) || !std::isfinite(fx) || !std::isfinite(fy)) return VISAR_INVALID_ARGUMENT;
+      // Tap tables depend only on (source, destination) lengths per axis:
+      // images of equal sizes share one device table (read only).
+      std::map<std::tuple<int, int, int, int>, const void *> tabs;  // (f32, axis, src, dst)
+      auto table_of = [&](bool f32, int axis, int sn, int dn) -> const void * {
+        const auto key = std::make_tuple(f32 ? 1 : 0, axis, sn, dn);
+        auto it = tabs.find(key);
+        if (it != tabs.end()) return it->second;
+        const void *t;
+        if (f32) {
+          std::vector<FLinTap> v(dn);
+          for (int k = 0; k < dn; k++) v[k] = lin_tap_f(k, sn, dn, false, axis == 0);
+          t = B.table(v);
+        } else {
+          std::vector<LinTap> v(dn);
+          for (int k = 0; k < dn; k++) v[k] = lin_tap_u8(k, sn, dn, false, axis == 0);
+          t = B.table(v);
+        }
+        tabs.emplace(key, t);
+        return t;
+      };
       for (size_t i = 0; i < n; i++) {
         const Buf &im = cur[i];
         const double wd = std::floor((double)im.v.w * fx), hd = std::floor((double)im.v.h * fy);
@@ -571,12 +611,9 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
         if (!B.image(dw, dh, im.v.cn, im.depth, next[i])) return VISAR_OUT_OF_MEMORY;
         const bool f32lin = im.depth == k32F && im.v.cn <= 4 && interp == 1;
         if (f32lin) {  // the generic f32 path (resize.zig:284-423), exact halves included
-          std::vector<FLinTap> xt(dw), yt(dh);
-          for (int x = 0; x < dw; x++) xt[x] = lin_tap_f(x, im.v.w, dw, false, true);
-          for (int y = 0; y < dh; y++) yt[y] = lin_tap_f(y, im.v.h, dh, false, false);
           BImg b = bimg(im.v, next[i].v);
-          b.t0 = B.table(xt);
-          b.t1 = B.table(yt);
+          b.t0 = table_of(true, 0, im.v.w, dw);
+          b.t1 = table_of(true, 1, im.v.h, dh);
           if (!B.sizing && (!b.t0 || !b.t1)) return VISAR_OUT_OF_MEMORY;
           Launch *l = class_of(ls, kOpLinear, k32F, im.v.cn, 0, false);
           add_img(l, b, im.input);
@@ -593,12 +630,9 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
           add_img(l, bimg(im.v, next[i].v), im.input);
           u8_bytes(*l, im.v, next[i].v, 1);
         } else {
-          std::vector<LinTap> xt(dw), yt(dh);
-          for (int x = 0; x < dw; x++) xt[x] = lin_tap_u8(x, im.v.w, dw, false, true);
-          for (int y = 0; y < dh; y++) yt[y] = lin_tap_u8(y, im.v.h, dh, false, false);
           BImg b = bimg(im.v, next[i].v);
-          b.t0 = B.table(xt);
-          b.t1 = B.table(yt);
+          b.t0 = table_of(false, 0, im.v.w, dw);
+          b.t1 = table_of(false, 1, im.v.h, dh);
           if (!B.sizing && (!b.t0 || !b.t1)) return VISAR_OUT_OF_MEMORY;
           Launch *l = class_of(ls, kOpLinear, k8U, im.v.cn, 0, false);
           add_img(l, b, im.input);

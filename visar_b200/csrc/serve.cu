@@ -467,6 +467,7 @@ struct visar_server {
       B.ext_alloc = &visar_server::pool_alloc;
       B.ext_ctx = &actx;
       Step step;
+      const double tb = now_s();
       int rc = build_stage(B, st, cur, next, step);
       // Descriptors, prefix sums and queue counters of the launches.
       std::vector<int *> counters;
@@ -485,6 +486,7 @@ struct visar_server {
           counters.push_back(c);
         }
       }
+      stats.build_s += now_s() - tb;
       size_t stage_bytes = 0;
       for (const Builder::Upload &u : B.uploads) stage_bytes += (u.data.size() + 255) & ~(size_t)255;
       uint8_t *stg = nullptr;
@@ -523,12 +525,15 @@ struct visar_server {
         const cudaStream_t gs = streams[gstream];
         gstream = (gstream + 1) % (int)streams.size();
         for (cudaEvent_t e : waits) cudaStreamWaitEvent(gs, e, 0);
+        const double tu = now_s();
         size_t off = 0;
         for (const Builder::Upload &u : B.uploads) {
           std::memcpy(stg + off, u.data.data(), u.data.size());
           cudaMemcpyAsync(u.dst, stg + off, u.data.size(), cudaMemcpyHostToDevice, gs);
           off += (u.data.size() + 255) & ~(size_t)255;
         }
+        const double tl = now_s();
+        stats.upload_s += tl - tu;
         for (size_t j = 0; j < step.launches.size(); j++) {
           Launch &L = step.launches[j];
           cudaMemsetAsync(counters[j], 0, sizeof(int), gs);
@@ -547,6 +552,7 @@ struct visar_server {
             }
           }
         }
+        stats.launch_s += now_s() - tl;
         gev = get_event();
         cudaEventRecord(gev, gs);
         cudaStreamWaitEvent(ls, gev, 0);
@@ -708,9 +714,11 @@ struct visar_server {
         poll_rounds();
         admit();
         if (broken.empty() && (int)rounds.size() < cfg.max_inflight) {
+          const double t0 = now_s();
           if (cfg.mode == VISAR_SERVE_PLAIN) did = launch_plain();
           else if (incoming.empty() && solo()) did = launch_plain(true);
           else did = launch_round();
+          if (did) stats.schedule_s += now_s() - t0;
         }
       }
       if (!did) std::this_thread::sleep_for(std::chrono::microseconds(20));
@@ -727,7 +735,7 @@ int visar_server_create(const visar_server_config *cfg, visar_server **out) {
   if (!s) return report_error(VISAR_OUT_OF_MEMORY, "OutOfMemory");
   if (cfg) s->cfg = *cfg;
   if (s->cfg.pool_bytes == 0) s->cfg.pool_bytes = (size_t)64 << 30;
-  if (s->cfg.max_inflight <= 0) s->cfg.max_inflight = 4;
+  if (s->cfg.max_inflight <= 0) s->cfg.max_inflight = 2;
   if (s->cfg.streams <= 0) s->cfg.streams = 8;
   if (s->cfg.mode != VISAR_SERVE_BATCHED && s->cfg.mode != VISAR_SERVE_PLAIN)
     return report_error(VISAR_INVALID_ARGUMENT, "InvalidArgument: serve mode");

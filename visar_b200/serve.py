@@ -26,7 +26,9 @@ class ServerStats(ctypes.Structure):
     _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("released", ctypes.c_uint64),
                 ("rounds", ctypes.c_uint64), ("launches", ctypes.c_uint64), ("fallback_calls", ctypes.c_uint64),
                 ("pool_bytes", ctypes.c_size_t), ("pool_used", ctypes.c_size_t), ("pool_reserved", ctypes.c_size_t),
-                ("mean_batch", ctypes.c_double), ("deferred", ctypes.c_uint64), ("solo", ctypes.c_uint64)]
+                ("mean_batch", ctypes.c_double), ("deferred", ctypes.c_uint64), ("solo", ctypes.c_uint64),
+                ("schedule_s", ctypes.c_double), ("build_s", ctypes.c_double), ("upload_s", ctypes.c_double),
+                ("launch_s", ctypes.c_double)]
 
 
 class TraceRequest(ctypes.Structure):
