@@ -208,6 +208,23 @@ def test_gauss_strip_every_border_and_edge_geometry():
         B.tune_load(None)
 
 
+def test_strips_on_strided_views():
+    """Caller images whose rows start 8-byte aligned but are not a multiple of
+    8 bytes long (views into wider buffers): the plan repacks them before the
+    strips, which read and write whole 8-byte words."""
+    imgs = []
+    for k, (h, w, c) in enumerate([(37, 19, 1), (70, 101, 3), (129, 45, 4), (64, 250, 1), (33, 7, 3)]):
+        pitch = ((w * c + 63) // 64) * 64 + 64
+        buf = torch.zeros((h, pitch), dtype=torch.uint8, device="cuda")
+        x = synth.base_image_torch(h, w, c, nrect=3, seed=900 + k)
+        v = buf[:, : w * c]
+        v.copy_(x.reshape(h, w * c))
+        imgs.append(v if c == 1 else v.view(h, w, c))
+    for spec in ([("gauss", {"k": (5, 5)})], [("gauss", {"k": (3, 3), "border": 1})],
+                 [("morph", {"op": 2, "shape": 2, "k": (5, 5)})], [("morph", {"op": 0, "shape": 0, "k": (3, 3)})]):
+        check_plan(imgs, spec)
+
+
 def test_every_strip_profile_fused_and_single():
     """Each compiled element profile (rect 3/5/7, cross 3/5, ellipse 5/7) as
     erode, dilate and the fused open / close, on 1-, 3- and 4-channel images."""

@@ -90,6 +90,7 @@ struct DevBuf {
   size_t cap = 0;
 };
 
+
 enum Slot { kSrc, kDst, kTmp1, kTmp2, kTmp3, kTmp4, kTab1, kTab2, kTab3, kTab4, kSmall, kNumSlots };
 
 struct DevCtx {
@@ -172,6 +173,8 @@ void *scratch(Call &call, Slot s, size_t bytes) {
 template <class T>
 T *upload(Call &call, Slot s, const std::vector<T> &v) {
   T *p = static_cast<T *>(scratch(call, s, v.size() * sizeof(T)));
+  // Tables are small: a copy from pageable memory costs the device less than
+  // a DMA from a pinned buffer would.
   if (!v.empty()) ck(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, call.st));
   return p;
 }
@@ -843,7 +846,7 @@ int visar_threshold(const visar_image *src, const visar_image *dst, double thres
         }
         host_lut[i] = o;
       }
-      ck(cudaMemcpyAsync(lut, host_lut.data(), 256, cudaMemcpyHostToDevice, call.st));
+      lut = upload(call, kTab1, host_lut);
       ck(launch_threshold_lut_u8(s.dev, d.dev, lut, call.st));
     } else if (depth == k32F) {
       ck(launch_threshold_cmp(s.dev, d.dev, depth, kind, (double)(float)thresh, (double)(float)maxval, call.st));
@@ -1093,10 +1096,8 @@ int visar_undistort(const visar_image *src, const visar_image *dst, const double
     if (s.c->channels < 1 || s.c->channels > 4) unsupported();
     double k8[8];
     expand_dist(dist, nd, k8);
-    std::vector<uint8_t> stripes;
-    const bool keeps_rows = undistort_stripes(k, k8, new_k, (int)s.c->width, (int)s.c->height, stripes);
+    const bool keeps_rows = undistort_any_singular(new_k, k, (int)s.c->width, (int)s.c->height);
     Call call = begin_call();
-    const void *tab = upload(call, kTab1, stripes);
     stage_in(call, s, kSrc);
     if (d.host && keeps_rows) {
       // Rows under a singular stripe camera are left as they are: start from dst.
@@ -1107,7 +1108,7 @@ int visar_undistort(const visar_image *src, const visar_image *dst, const double
       stage_out(call, d, kDst);
     }
     if (overlaps(s, d)) detach_src(call, s, kTmp1);
-    ck(launch_undistort(s.dev, d.dev, tab, call.st));
+    ck(launch_undistort(s.dev, d.dev, k, k8, new_k, call.st));
     finish_out(call, d);
     end_call(call, s.host || d.host);
   });

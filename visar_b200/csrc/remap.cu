@@ -58,24 +58,107 @@ __device__ __forceinline__ void map_px(const UndistParams &p, double i, double j
   v = __dadd_rn(__dmul_rn(p.fy, yd), p.v0);
 }
 
-// OpenCV's saturate_cast<int>(v * 32): clamped, rounded half to even.
+// OpenCV's saturate_cast<int>(v * 32): clamped, rounded half to even. The
+// rounding is an add of 1.5 * 2^52 (exact for |s| < 2^51, the sum's low word
+// then holds the integer): the same value as __double2int_rn without the
+// conversion unit.
 __device__ __forceinline__ int fix32(double v) {
   const double s = fmin(fmax(__dmul_rn(v, 32.0), -2147483647.0), 2147483647.0);
-  return __double2int_rn(s);
+  return (int)__double2loint(__dadd_rn(s, 6755399441055744.0));
+}
+
+// The camera of an undistort stripe: the inverse of the new camera matrix
+// with its principal point moved up by the stripe's first row, as
+// linalg.inv3 computes it (src/calib3d/linalg.zig:417-426; the host restatement
+// inv3 below evaluates the same expressions in the same order, each product
+// and sum rounded on its own, 1 / det correctly rounded).
+struct UndistBase {
+  double ar[9];  // the new camera matrix (new_k, else K)
+  double fx, fy, u0, v0;
+  double k[8];
+  bool ratio;
+};
+
+__device__ __forceinline__ double dif2(double a, double b, double c, double d) {
+  return __dsub_rn(__dmul_rn(a, b), __dmul_rn(c, d));  // a*b - c*d
+}
+
+__device__ void stripe_params(const UndistBase &b, int first_row, UndistParams &p) {
+  double a[9];
+#pragma unroll
+  for (int i = 0; i < 9; i++) a[i] = b.ar[i];
+  a[5] = __dsub_rn(b.ar[5], (double)first_row);
+  const double det = __dadd_rn(__dsub_rn(__dmul_rn(a[0], dif2(a[4], a[8], a[7], a[5])), __dmul_rn(a[1], dif2(a[3], a[8], a[6], a[5]))),
+                               __dmul_rn(a[2], dif2(a[3], a[7], a[6], a[4])));
+  p.fx = b.fx;
+  p.fy = b.fy;
+  p.u0 = b.u0;
+  p.v0 = b.v0;
+#pragma unroll
+  for (int i = 0; i < 8; i++) p.k[i] = b.k[i];
+  p.ratio = b.ratio;
+  p.skip = det == 0;
+  if (p.skip) {
+    p.persp = false;
+    return;
+  }
+  const double d = __drcp_rn(det);
+  p.ir[0] = __dmul_rn(dif2(a[4], a[8], a[5], a[7]), d);
+  p.ir[1] = __dmul_rn(dif2(a[2], a[7], a[1], a[8]), d);
+  p.ir[2] = __dmul_rn(dif2(a[1], a[5], a[2], a[4]), d);
+  p.ir[3] = __dmul_rn(dif2(a[5], a[6], a[3], a[8]), d);
+  p.ir[4] = __dmul_rn(dif2(a[0], a[8], a[2], a[6]), d);
+  p.ir[5] = __dmul_rn(dif2(a[2], a[3], a[0], a[5]), d);
+  p.ir[6] = __dmul_rn(dif2(a[3], a[7], a[4], a[6]), d);
+  p.ir[7] = __dmul_rn(dif2(a[1], a[6], a[0], a[7]), d);
+  p.ir[8] = __dmul_rn(dif2(a[0], a[4], a[1], a[3]), d);
+  p.persp = !(p.ir[6] == 0 && p.ir[7] == 0 && p.ir[8] == 1);
+}
+
+// The CN bytes of pixel x and of pixel x + 1 of row r. 3- and 4-channel
+// rows with 8-byte aligned starts (`wide`) take two aligned 8-byte loads
+// when the 16-byte window stays inside the row, and pick the bytes by
+// permutes; otherwise bytewise.
+template <int CN>
+__device__ __forceinline__ void tap_pair(const uint8_t *r, int x, int row_bytes, bool wide, int (&p)[CN], int (&q)[CN]) {
+  if constexpr (CN == 3 || CN == 4) {
+    const int b = x * CN, a8 = b & ~7;
+    if (wide && a8 + 16 <= row_bytes) {
+      const uint2 lo = __ldg(reinterpret_cast<const uint2 *>(r + a8));
+      const uint2 hi = __ldg(reinterpret_cast<const uint2 *>(r + a8 + 8));
+      const int off = b - a8;  // 0..7
+      const uint32_t wa = off >= 4 ? lo.y : lo.x, wb = off >= 4 ? hi.x : lo.y, wc = off >= 4 ? hi.y : hi.x;
+      const unsigned sel = 0x3210u + 0x1111u * (unsigned)(off & 3);
+      const uint32_t b0 = __byte_perm(wa, wb, sel), b1 = __byte_perm(wb, wc, sel);  // bytes off .. off + 7
+#pragma unroll
+      for (int c = 0; c < CN; c++) {
+        p[c] = (int)((b0 >> (8 * c)) & 0xFFu);
+        const int k = c + CN;
+        q[c] = (int)(((k < 4 ? b0 : b1) >> (8 * (k & 3))) & 0xFFu);
+      }
+      return;
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < CN; c++) {
+    p[c] = r[x * CN + c];
+    q[c] = r[x * CN + CN + c];
+  }
 }
 
 template <int CN>
 __device__ __forceinline__ void sample_fixed(const uint8_t *__restrict__ src, long long stride, int W, int H, int iu, int iv,
-                                             uint8_t *o) {
+                                             uint8_t *o, bool wide = false) {
   const int sx = iu >> 5, sy = iv >> 5;
   const int a = iu & 31, b = iv & 31;
   const int w0 = (32 - a) * (32 - b), w1 = a * (32 - b), w2 = (32 - a) * b, w3 = a * b;
   if (sx >= 0 && sx < W - 1 && sy >= 0 && sy < H - 1) {
-    const uint8_t *p0 = src + (long long)sy * stride + (long long)sx * CN;
-    const uint8_t *p1 = p0 + stride;
+    const uint8_t *r0 = src + (long long)sy * stride;
+    int p0[CN], q0[CN], p1[CN], q1[CN];
+    tap_pair<CN>(r0, sx, W * CN, wide, p0, q0);
+    tap_pair<CN>(r0 + stride, sx, W * CN, wide, p1, q1);
 #pragma unroll
-    for (int c = 0; c < CN; c++)
-      o[c] = (uint8_t)(((int)p0[c] * w0 + (int)p0[c + CN] * w1 + (int)p1[c] * w2 + (int)p1[c + CN] * w3 + 512) >> 10);
+    for (int c = 0; c < CN; c++) o[c] = (uint8_t)((p0[c] * w0 + q0[c] * w1 + p1[c] * w2 + q1[c] * w3 + 512) >> 10);
     return;
   }
   if (sx >= W || sx + 1 < 0 || sy >= H || sy + 1 < 0) {
@@ -97,24 +180,46 @@ __device__ __forceinline__ void sample_fixed(const uint8_t *__restrict__ src, lo
   }
 }
 
-// undistort: one thread per destination pixel; the stripe's parameters come
-// from the table built on the host (one entry per stripe).
+// undistort: four consecutive destination pixels per thread (their map
+// arithmetic and taps interleave); a block of 32 x 8 threads covers 8 rows,
+// whose stripes' cameras (at most 8) its first threads compute into shared
+// memory.
+constexpr int kUndRows = 8;
+
 template <int CN>
-__global__ void k_undistort(const uint8_t *__restrict__ src, long long sstride, uint8_t *__restrict__ dst, long long dstride,
-                            int W, int H, int stripe, const UndistParams *__restrict__ stripes) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  if (x >= W || y >= H) return;
+__global__ void __launch_bounds__(256) k_undistort(const uint8_t *__restrict__ src, long long sstride, uint8_t *__restrict__ dst,
+                                                   long long dstride, int W, int H, int stripe, UndistBase base, int wide) {
+  __shared__ UndistParams sp[kUndRows];
+  const int y0 = blockIdx.y * kUndRows;
+  const int s0 = y0 / stripe, s1 = min(y0 + kUndRows - 1, H - 1) / stripe;
+  const int t = threadIdx.y * blockDim.x + threadIdx.x;
+  if (t <= s1 - s0) stripe_params(base, (s0 + t) * stripe, sp[t]);
+  __syncthreads();
+  const int x0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
+  const int y = y0 + threadIdx.y;
+  if (x0 >= W || y >= H) return;
   const int s = y / stripe;
-  const UndistParams &p = stripes[s];
-  uint8_t *o = dst + (long long)y * dstride + (long long)x * CN;
+  const UndistParams &p = sp[s - s0];
   if (p.skip) return;
-  double u, v;
-  map_px(p, (double)(y - s * stripe), (double)x, u, v);
-  uint8_t px[CN];
-  sample_fixed<CN>(src, sstride, W, H, fix32(u), fix32(v), px);
+  const double i = (double)(y - s * stripe);
+  uint8_t *o = dst + (long long)y * dstride + (long long)x0 * CN;
+  int iu[4], iv[4];
 #pragma unroll
-  for (int c = 0; c < CN; c++) o[c] = px[c];
+  for (int q = 0; q < 4; q++) {
+    double u, v;
+    map_px(p, i, (double)(x0 + q), u, v);
+    iu[q] = fix32(u);
+    iv[q] = fix32(v);
+  }
+  uint8_t px[4][CN];
+#pragma unroll
+  for (int q = 0; q < 4; q++) sample_fixed<CN>(src, sstride, W, H, iu[q], iv[q], px[q], wide != 0);
+#pragma unroll
+  for (int q = 0; q < 4; q++)
+    if (x0 + q < W) {
+#pragma unroll
+      for (int c = 0; c < CN; c++) o[q * CN + c] = px[q][c];
+    }
 }
 
 __global__ void k_init_map(float *__restrict__ mx, long long mxs, float *__restrict__ my, long long mys, int W, int H,
@@ -205,27 +310,22 @@ int undistort_stripe_rows(int width, int height) {
   return std::min(s, height);
 }
 
-bool undistort_stripes(const double K[9], const double k8[8], const double *new_k, int width, int height,
-                       std::vector<uint8_t> &out) {
-  bool any_skip = false;
+bool undistort_any_singular(const double *new_k, const double K[9], int width, int height) {
+  // The stripes' cameras (inverted on the device): singular when det = 0,
+  // which, as det is linear in the principal point, is at most one stripe
+  // (or every stripe).
   const int stripe = undistort_stripe_rows(width, height);
   const int n = (height + stripe - 1) / stripe;
-  out.assign((size_t)n * sizeof(UndistParams), 0);
-  UndistParams *ps = reinterpret_cast<UndistParams *>(out.data());
   const double *ar0 = new_k ? new_k : K;
   for (int s = 0; s < n; s++) {
-    double ar[9], ir[9];
-    for (int i = 0; i < 9; i++) ar[i] = ar0[i];
-    ar[5] = ar0[5] - (double)(s * stripe);
-    if (!inv3(ar, ir)) {
-      fill_params(ps[s], ar, K, k8);
-      ps[s].skip = true;
-      any_skip = true;
-      continue;
-    }
-    fill_params(ps[s], ir, K, k8);
+    double a[9];
+    for (int i = 0; i < 9; i++) a[i] = ar0[i];
+    a[5] = ar0[5] - (double)(s * stripe);
+    const double det =
+        a[0] * (a[4] * a[8] - a[7] * a[5]) - a[1] * (a[3] * a[8] - a[6] * a[5]) + a[2] * (a[3] * a[7] - a[6] * a[4]);
+    if (det == 0) return true;
   }
-  return any_skip;
+  return false;
 }
 
 bool undistort_map_params(const double K[9], const double k8[8], const double *R, const double *new_k, std::vector<uint8_t> &out) {
@@ -238,16 +338,26 @@ bool undistort_map_params(const double K[9], const double k8[8], const double *R
   return true;
 }
 
-cudaError_t launch_undistort(const DImg &s, const DImg &d, const void *stripes_dev, cudaStream_t st) {
+cudaError_t launch_undistort(const DImg &s, const DImg &d, const double K[9], const double k8[8], const double *new_k,
+                             cudaStream_t st) {
   const int stripe = undistort_stripe_rows(s.w, s.h);
-  dim3 block(32, 8), grid((d.w + 31) / 32, (d.h + 7) / 8);
-  const UndistParams *ps = static_cast<const UndistParams *>(stripes_dev);
+  UndistBase b{};
+  const double *ar0 = new_k ? new_k : K;
+  for (int i = 0; i < 9; i++) b.ar[i] = ar0[i];
+  b.fx = K[0];
+  b.fy = K[4];
+  b.u0 = K[2];
+  b.v0 = K[5];
+  for (int i = 0; i < 8; i++) b.k[i] = k8[i];
+  b.ratio = k8[5] != 0 || k8[6] != 0 || k8[7] != 0;
+  const int wide = ((uintptr_t)s.p % 8 == 0) && (s.stride % 8 == 0);
+  dim3 block(32, kUndRows), grid((d.w + 127) / 128, (d.h + kUndRows - 1) / kUndRows);
   note_launch();
   switch (s.cn) {
-    case 1: k_undistort<1><<<grid, block, 0, st>>>(s.p, s.stride, d.p, d.stride, s.w, s.h, stripe, ps); break;
-    case 2: k_undistort<2><<<grid, block, 0, st>>>(s.p, s.stride, d.p, d.stride, s.w, s.h, stripe, ps); break;
-    case 3: k_undistort<3><<<grid, block, 0, st>>>(s.p, s.stride, d.p, d.stride, s.w, s.h, stripe, ps); break;
-    default: k_undistort<4><<<grid, block, 0, st>>>(s.p, s.stride, d.p, d.stride, s.w, s.h, stripe, ps); break;
+    case 1: k_undistort<1><<<grid, block, 0, st>>>(s.p, s.stride, d.p, d.stride, s.w, s.h, stripe, b, wide); break;
+    case 2: k_undistort<2><<<grid, block, 0, st>>>(s.p, s.stride, d.p, d.stride, s.w, s.h, stripe, b, wide); break;
+    case 3: k_undistort<3><<<grid, block, 0, st>>>(s.p, s.stride, d.p, d.stride, s.w, s.h, stripe, b, wide); break;
+    default: k_undistort<4><<<grid, block, 0, st>>>(s.p, s.stride, d.p, d.stride, s.w, s.h, stripe, b, wide); break;
   }
   return cudaGetLastError();
 }

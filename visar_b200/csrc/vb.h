@@ -123,12 +123,13 @@ cudaError_t launch_pyr_up(const DImg &s, const DImg &d, int depth, cudaStream_t 
 // byte vectors (one per stripe of undistort's rows, or one for the map) and
 // passed as device copies (undistort) or by value (the map).
 int undistort_stripe_rows(int width, int height);
-// Returns true when some stripe's camera matrix is singular (its rows are left as they are).
-bool undistort_stripes(const double K[9], const double k8[8], const double *new_k, int width, int height,
-                       std::vector<uint8_t> &out);
+// True when the camera of some undistort stripe is singular (its rows are
+// then left as they are).
+bool undistort_any_singular(const double *new_k, const double K[9], int width, int height);
 bool undistort_map_params(const double K[9], const double k8[8], const double *R, const double *new_k,
                           std::vector<uint8_t> &out);
-cudaError_t launch_undistort(const DImg &s, const DImg &d, const void *stripes_dev, cudaStream_t st);
+cudaError_t launch_undistort(const DImg &s, const DImg &d, const double K[9], const double k8[8], const double *new_k,
+                             cudaStream_t st);
 cudaError_t launch_init_undistort_map(const std::vector<uint8_t> &params, const DImg &mx, const DImg &my, cudaStream_t st);
 cudaError_t launch_remap(const DImg &s, const DImg &d, const DImg &mx, const DImg &my, uint8_t value, cudaStream_t st);
 
