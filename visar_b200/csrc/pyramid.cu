@@ -59,10 +59,12 @@ constexpr int kThreads = 256;
 
 // pyrDown tile: output rows [oy0, oy0 + kDownRows), output pixels [ox0, ox0 + twp).
 // CN_: the channel count when compiled in (1, 3, 4), else 0 (cn at run time).
+// vec: u8 destination rows 4-byte aligned and tiles of a multiple of 4
+// output pixels; svec: source rows 4-byte aligned.
 template <class T, int CN_>
 __global__ void __launch_bounds__(kThreads) k_pyr_down(const uint8_t *__restrict__ src, long long sstride, int sw, int sh,
                                                        uint8_t *__restrict__ dst, long long dstride, int dw, int dh,
-                                                       int cn_rt, int twp, int border) {
+                                                       int cn_rt, int twp, int border, int vec, int svec) {
   using A = typename PyrAcc<T>::A;
   const int cn = CN_ > 0 ? CN_ : cn_rt;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -82,8 +84,42 @@ __global__ void __launch_bounds__(kThreads) k_pyr_down(const uint8_t *__restrict
   const bool inner = 2 * ox0 - 2 >= 0 && 2 * (ox0 + npx - 1) + 2 < sw;
   const int e0 = (2 * ox0 - 2) * cn;
   // Phase 1: vertical sums, V[r * span + e]; every row of a column is loaded
-  // before the sums, so the loads are in flight together.
-  for (int e = threadIdx.x; e < span; e += kThreads) {
+  // before the sums, so the loads are in flight together. u8 inner tiles
+  // whose words stay inside the row take 4 bytes per thread and row (32-bit
+  // loads from 4-byte aligned rows), summed as two 16-bit pair lanes
+  // (sums <= 255 * 16, no carry between lanes).
+  bool done = false;
+  if constexpr (sizeof(T) == 1) {
+    const int w0 = e0 & ~3;
+    const int nw = (e0 + span - w0 + 3) >> 2;
+    if (svec && inner && w0 + 4 * nw <= sw * cn) {
+      for (int wi = threadIdx.x; wi < nw; wi += kThreads) {
+        const int wb = w0 + 4 * wi;
+        uint32_t r[NS];
+#pragma unroll
+        for (int k = 0; k < NS; k++) r[k] = k < 2 * nrows + 3 ? *reinterpret_cast<const uint32_t *>(s_row[k] + wb) : 0u;
+        const int e = wb - e0;  // span element of the word's byte 0
+#pragma unroll
+        for (int rr = 0; rr < kDownRows; rr++) {
+          if (rr >= nrows) break;
+          uint32_t lo[5], hi[5];
+#pragma unroll
+          for (int t = 0; t < 5; t++) {
+            lo[t] = r[2 * rr + t] & 0x00FF00FFu;         // bytes 0, 2
+            hi[t] = (r[2 * rr + t] >> 8) & 0x00FF00FFu;  // bytes 1, 3
+          }
+          const uint32_t sl = ((lo[0] + lo[4]) + (lo[1] + lo[3]) * 4u) + lo[2] * 6u;
+          const uint32_t sh8 = ((hi[0] + hi[4]) + (hi[1] + hi[3]) * 4u) + hi[2] * 6u;
+          const int v4[4] = {(int)(sl & 0xFFFFu), (int)(sh8 & 0xFFFFu), (int)(sl >> 16), (int)(sh8 >> 16)};
+#pragma unroll
+          for (int b = 0; b < 4; b++)
+            if (e + b >= 0 && e + b < span) V[rr * span + e + b] = v4[b];
+        }
+      }
+      done = true;
+    }
+  }
+  for (int e = threadIdx.x; e < span && !done; e += kThreads) {
     int se = e0 + e;
     if (!inner) {
       const int px = 2 * ox0 - 2 + e / cn;
@@ -98,6 +134,41 @@ __global__ void __launch_bounds__(kThreads) k_pyr_down(const uint8_t *__restrict
   }
   __syncthreads();
   // Phase 2: output element j of the tile row sits over padded element 2j - j % cn + 2cn.
+  if constexpr (sizeof(T) == 1 && CN_ > 0) {
+    if (vec) {
+      // u8: per thread and output row, four output pixels 4g .. 4g + 3 of
+      // the tile (4 * CN bytes, CN aligned 32-bit stores); output element j
+      // sits over padded element 2j - j % CN + 2CN.
+      constexpr int CN = CN_;
+      const int ng = (npx + 3) >> 2;
+      for (int t = threadIdx.x; t < nrows * ng; t += kThreads) {
+        const int r = t / ng, g = t - r * ng;
+        const A *v = V + r * span + (8 * g + 2) * CN;  // output pixel 4g's channel 0
+        const int npo = min(4, npx - 4 * g);
+        uint32_t w[CN];
+#pragma unroll
+        for (int k = 0; k < CN; k++) w[k] = 0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          if (k >= npo) break;
+#pragma unroll
+          for (int c = 0; c < CN; c++) {
+            const A *x = v + 2 * k * CN + c;
+            const int byte = k * CN + c;
+            w[byte >> 2] |= (uint32_t)pyr_finish<T, 8>(tap5(x[-2 * CN], x[-CN], x[0], x[CN], x[2 * CN])) << (8 * (byte & 3));
+          }
+        }
+        uint8_t *o = dst + (long long)(oy0 + r) * dstride + (long long)(ox0 + 4 * g) * CN;
+        if (npo == 4) {
+#pragma unroll
+          for (int k = 0; k < CN; k++) reinterpret_cast<uint32_t *>(o)[k] = w[k];
+        } else {
+          for (int b = 0; b < npo * CN; b++) o[b] = (uint8_t)(w[b >> 2] >> (8 * (b & 3)));
+        }
+      }
+      return;
+    }
+  }
   const int ne = npx * cn;
   for (int r = 0; r < nrows; r++) {
     T *orow = reinterpret_cast<T *>(dst + (long long)(oy0 + r) * dstride) + (long long)ox0 * cn;
@@ -135,9 +206,11 @@ constexpr int kUpRows = 8;  // source rows per tile (16 output rows)
 __device__ __forceinline__ int up_row(int y, int h) { return y < 0 ? (h > 1 ? 1 : 0) : y >= h ? h - 1 : y; }
 
 // pyrUp tile: source rows [sy0, sy0 + kUpRows), source pixels [sx0, sx0 + twp).
+// vec: u8 destination rows 4-byte aligned (tiles start on 4-byte boundaries:
+// 2 * twp * cn is a multiple of 4).
 template <class T, int CN_>
 __global__ void __launch_bounds__(kThreads) k_pyr_up(const uint8_t *__restrict__ src, long long sstride, int sw, int sh,
-                                                     uint8_t *__restrict__ dst, long long dstride, int cn_rt, int twp) {
+                                                     uint8_t *__restrict__ dst, long long dstride, int cn_rt, int twp, int vec) {
   using A = typename PyrAcc<T>::A;
   const int cn = CN_ > 0 ? CN_ : cn_rt;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -174,6 +247,44 @@ __global__ void __launch_bounds__(kThreads) k_pyr_up(const uint8_t *__restrict__
     }
   }
   __syncthreads();
+  if constexpr (sizeof(T) == 1 && CN_ > 0) {
+    if (vec) {
+      constexpr int CN = CN_;
+      // u8: per thread and output row, the four output pixels over source
+      // pixels p0 = 2g and p0 + 1 of the tile (4 * CN bytes, CN aligned
+      // 32-bit stores); q[k * CN + c] is source pixel p0 + k, k = -1 .. 2.
+      const int ng = (npx + 1) >> 1;
+      for (int t = threadIdx.x; t < 2 * nrows * ng; t += kThreads) {
+        const int rr = t / ng, g = t - rr * ng;
+        const A *q = ((rr & 1) ? O : E) + (rr >> 1) * span + (2 * g + 1) * CN;
+        const int npo = min(4, 2 * npx - 4 * g);  // output pixels of the group inside the tile (4 or 2)
+        uint32_t w[CN];
+#pragma unroll
+        for (int k = 0; k < CN; k++) w[k] = 0;
+#pragma unroll
+        for (int op = 0; op < 4; op++) {
+          if (op >= npo) break;
+          const int pp = op >> 1;
+#pragma unroll
+          for (int c = 0; c < CN; c++) {
+            const A s = (op & 1) ? up_odd(q[pp * CN + c], q[(pp + 1) * CN + c])
+                                 : up_even(q[(pp - 1) * CN + c], q[pp * CN + c], q[(pp + 1) * CN + c]);
+            const int byte = op * CN + c;
+            w[byte >> 2] |= (uint32_t)pyr_finish<T, 6>(s) << (8 * (byte & 3));
+          }
+        }
+        uint8_t *o = dst + (long long)(2 * sy0 + rr) * dstride + (long long)(2 * sx0 + 4 * g) * CN;
+        if (npo == 4) {
+#pragma unroll
+          for (int k = 0; k < CN; k++) reinterpret_cast<uint32_t *>(o)[k] = w[k];
+        } else {
+#pragma unroll
+          for (int b = 0; b < 2 * CN; b++) o[b] = (uint8_t)(w[b >> 2] >> (8 * (b & 3)));
+        }
+      }
+      return;
+    }
+  }
   // Output pixel 2p (+1) of tile row r; q[p] is smem element (p - sx0 + 1) * cn.
   const int ne = 2 * npx * cn;
   for (int rr = 0; rr < 2 * nrows; rr++) {  // output row within the tile
@@ -221,14 +332,17 @@ cudaError_t pyr_down_t(const DImg &s, const DImg &d, int border, cudaStream_t st
     k_pyr_down_direct<T><<<blocks, 256, 0, st>>>(s.p, s.stride, s.w, s.h, d.p, d.stride, d.w, d.h, s.cn, border);
     return cudaGetLastError();
   }
-  const int twp = std::max(1, kDownElems / s.cn);
+  // Tiles of a multiple of 4 output pixels (4-byte aligned u8 tile rows).
+  const int twp = std::max(4, (kDownElems / s.cn) & ~3);
   const size_t smem = (size_t)kDownRows * (2 * twp + 3) * s.cn * sizeof(A);
   dim3 grid((d.w + twp - 1) / twp, (d.h + kDownRows - 1) / kDownRows);
+  const int vec = (uintptr_t)d.p % 4 == 0 && d.stride % 4 == 0;
+  const int svec = (uintptr_t)s.p % 4 == 0 && s.stride % 4 == 0;
   switch (s.cn) {
-    case 1: k_pyr_down<T, 1><<<grid, kThreads, smem, st>>>(s.p, s.stride, s.w, s.h, d.p, d.stride, d.w, d.h, 1, twp, border); break;
-    case 3: k_pyr_down<T, 3><<<grid, kThreads, smem, st>>>(s.p, s.stride, s.w, s.h, d.p, d.stride, d.w, d.h, 3, twp, border); break;
-    case 4: k_pyr_down<T, 4><<<grid, kThreads, smem, st>>>(s.p, s.stride, s.w, s.h, d.p, d.stride, d.w, d.h, 4, twp, border); break;
-    default: k_pyr_down<T, 0><<<grid, kThreads, smem, st>>>(s.p, s.stride, s.w, s.h, d.p, d.stride, d.w, d.h, s.cn, twp, border);
+    case 1: k_pyr_down<T, 1><<<grid, kThreads, smem, st>>>(s.p, s.stride, s.w, s.h, d.p, d.stride, d.w, d.h, 1, twp, border, vec, svec); break;
+    case 3: k_pyr_down<T, 3><<<grid, kThreads, smem, st>>>(s.p, s.stride, s.w, s.h, d.p, d.stride, d.w, d.h, 3, twp, border, vec, svec); break;
+    case 4: k_pyr_down<T, 4><<<grid, kThreads, smem, st>>>(s.p, s.stride, s.w, s.h, d.p, d.stride, d.w, d.h, 4, twp, border, vec, svec); break;
+    default: k_pyr_down<T, 0><<<grid, kThreads, smem, st>>>(s.p, s.stride, s.w, s.h, d.p, d.stride, d.w, d.h, s.cn, twp, border, vec, svec);
   }
   return cudaGetLastError();
 }
@@ -246,11 +360,12 @@ cudaError_t pyr_up_t(const DImg &s, const DImg &d, cudaStream_t st) {
   const int twp = std::max(1, 128 / s.cn);
   const size_t smem = (size_t)2 * kUpRows * (twp + 2) * s.cn * sizeof(A);
   dim3 grid((s.w + twp - 1) / twp, (s.h + kUpRows - 1) / kUpRows);
+  const int vec = (uintptr_t)d.p % 4 == 0 && d.stride % 4 == 0 && (2 * twp * s.cn) % 4 == 0;
   switch (s.cn) {
-    case 1: k_pyr_up<T, 1><<<grid, kThreads, smem, st>>>(s.p, s.stride, s.w, s.h, d.p, d.stride, 1, twp); break;
-    case 3: k_pyr_up<T, 3><<<grid, kThreads, smem, st>>>(s.p, s.stride, s.w, s.h, d.p, d.stride, 3, twp); break;
-    case 4: k_pyr_up<T, 4><<<grid, kThreads, smem, st>>>(s.p, s.stride, s.w, s.h, d.p, d.stride, 4, twp); break;
-    default: k_pyr_up<T, 0><<<grid, kThreads, smem, st>>>(s.p, s.stride, s.w, s.h, d.p, d.stride, s.cn, twp);
+    case 1: k_pyr_up<T, 1><<<grid, kThreads, smem, st>>>(s.p, s.stride, s.w, s.h, d.p, d.stride, 1, twp, vec); break;
+    case 3: k_pyr_up<T, 3><<<grid, kThreads, smem, st>>>(s.p, s.stride, s.w, s.h, d.p, d.stride, 3, twp, vec); break;
+    case 4: k_pyr_up<T, 4><<<grid, kThreads, smem, st>>>(s.p, s.stride, s.w, s.h, d.p, d.stride, 4, twp, vec); break;
+    default: k_pyr_up<T, 0><<<grid, kThreads, smem, st>>>(s.p, s.stride, s.w, s.h, d.p, d.stride, s.cn, twp, vec);
   }
   return cudaGetLastError();
 }
