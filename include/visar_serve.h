@@ -33,7 +33,7 @@ enum visar_serve_mode { VISAR_SERVE_BATCHED = 0, VISAR_SERVE_PLAIN = 1 };
 typedef struct visar_server_config {
     size_t pool_bytes;   /* device pool for intermediate and final results (0: 64 GiB) */
     int mode;            /* enum visar_serve_mode */
-    int max_inflight;    /* scheduling rounds queued on the GPU at once (0: 2; fewer rounds in flight make larger groups) */
+    int max_inflight;    /* scheduling rounds queued on the GPU at once (0: 4; at most 2 while 256 or more requests wait, so that they form larger groups) */
     int streams;         /* streams the stage groups of a round spread over (0: 8) */
 } visar_server_config;
 

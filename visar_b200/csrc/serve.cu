@@ -181,6 +181,10 @@ struct Trace {
   std::string first_error;
 };
 
+// Requests waiting or admitted from which a scheduling round keeps at most
+// two rounds in flight.
+constexpr size_t kBacklog = 256;
+
 struct Round {
   // ev_launch: every launch of the round is done (each stage group runs on
   // a stream of its own and records a group event, in groups); ev_fb: its
@@ -713,7 +717,11 @@ struct visar_server {
         if (!broken.empty() && !incoming.empty()) fail_all(cudaSuccess);
         poll_rounds();
         admit();
-        if (broken.empty() && (int)rounds.size() < cfg.max_inflight) {
+        // A long backlog takes fewer rounds in flight, so that more requests
+        // gather per round (larger groups); a short one takes the configured
+        // number, which keeps the latency of moderate loads low.
+        const int limit = incoming.size() + admitted.size() >= kBacklog ? std::min(cfg.max_inflight, 2) : cfg.max_inflight;
+        if (broken.empty() && (int)rounds.size() < limit) {
           const double t0 = now_s();
           if (cfg.mode == VISAR_SERVE_PLAIN) did = launch_plain();
           else if (incoming.empty() && solo()) did = launch_plain(true);
@@ -735,7 +743,7 @@ int visar_server_create(const visar_server_config *cfg, visar_server **out) {
   if (!s) return report_error(VISAR_OUT_OF_MEMORY, "OutOfMemory");
   if (cfg) s->cfg = *cfg;
   if (s->cfg.pool_bytes == 0) s->cfg.pool_bytes = (size_t)64 << 30;
-  if (s->cfg.max_inflight <= 0) s->cfg.max_inflight = 2;
+  if (s->cfg.max_inflight <= 0) s->cfg.max_inflight = 4;
   if (s->cfg.streams <= 0) s->cfg.streams = 8;
   if (s->cfg.mode != VISAR_SERVE_BATCHED && s->cfg.mode != VISAR_SERVE_PLAIN)
     return report_error(VISAR_INVALID_ARGUMENT, "InvalidArgument: serve mode");
