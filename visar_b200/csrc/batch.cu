@@ -282,20 +282,21 @@ void tune_and_tile(Launch &L, int num_sms) {
     }
     case kOpGaussStrip: case kOpMorphStrip: {
       // Warp tiles of 128 (one-channel images), 64 (Gaussian, one-channel
-      // morphology), 32 or 8 rows: by default the tallest of 64/32/8 that
-      // leaves ~8 tiles per resident warp slot (taller tiles re-read fewer
-      // halo rows); 128 when tuned.
+      // morphology), 32 or 8 rows: by default the tallest that leaves ~4
+      // (128 rows) or ~8 (shorter tiles) tiles per resident warp slot --
+      // taller tiles re-read fewer halo rows, and 128-row tiles save enough
+      // of them to outweigh a longer tail.
       const bool has64 = L.op == kOpGaussStrip || L.cn == 1;
       if (tuned == 8 || tuned == 32 || (tuned == 64 && has64) || (tuned == 128 && L.cn == 1)) {
         L.rows = tuned;
         retile();
         break;
       }
-      for (const int rh : {64, 32, 8}) {
-        if (rh == 64 && !has64) continue;
+      for (const int rh : {128, 64, 32, 8}) {
+        if ((rh == 64 && !has64) || (rh == 128 && L.cn != 1)) continue;
         L.rows = rh;
         retile();
-        if (total_tiles(L) >= 8LL * num_sms * 24) break;
+        if (total_tiles(L) >= (rh == 128 ? 4LL : 8LL) * num_sms * 24) break;
       }
       break;
     }
