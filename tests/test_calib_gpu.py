@@ -116,3 +116,25 @@ def test_refusals():
     with pytest.raises(vb.VisarError) as e:
         vb.remap(img, mx.to(torch.float16), mx.to(torch.float16))
     assert e.value.status == -3
+
+
+def test_undistort_singular_stripe_keeps_rows():
+    """A new camera matrix whose stripe camera is singular for one stripe
+    (det is linear in the principal point: 500 * (2 - a5) here, zero for the
+    stripe whose first row is cy - 2 = 20): those rows are left as they are,
+    the others follow the projective map (a camera with a perspective row).
+    The device inverts each stripe's camera as the oracle does."""
+    h, w = 64, 1024  # 4 rows per stripe
+    rng = np.random.default_rng(77)
+    img = rng.integers(0, 256, (h, w, 3), dtype=np.uint8)
+    K = np.array([[500.0, 0, 510], [0, 500.0, 30], [0, 0, 1]])
+    new_k = np.array([[500.0, 0, 510], [0, 2.0, 22.0], [0, 1.0, 1.0]])
+    dist = [-0.1, 0.01, 0.0, 0.0]
+    ref = O.undistort(img, K, dist, new_k, dst=np.full((h, w, 3), 77, np.uint8))
+    assert np.all(ref[20:24] == 77) and not np.all(ref == 77)
+    d_dst = dev(np.full((h, w, 3), 77, np.uint8))
+    vb.undistort(dev(img), K, dist, new_k, dst=d_dst)
+    assert np.array_equal(host(d_dst), ref)
+    h_dst = np.full((h, w, 3), 77, np.uint8)
+    vb.undistort(img, K, dist, new_k, dst=h_dst)
+    assert np.array_equal(h_dst, ref)
