@@ -723,7 +723,7 @@ struct NoArgs {
 // on warp strips (strip.cuh).
 template <class P1, class P2, int CN, int RH, bool MAX1, bool FUSED>
 struct OpMorphStrip {
-  static constexpr int kThreads = 128, kMinBlocks = FUSED && P1::KH >= 7 ? 4 : 6;  // <= 128 / 85 registers
+  static constexpr int kThreads = 128, kMinBlocks = FUSED && P1::KH >= 7 ? 4 : FUSED ? 5 : 6;  // <= 128 / 102 / 85 registers
   static constexpr bool kWarpTiles = true;
   using Args = NoArgs;
   static size_t smem(const Args &) { return 0; }

@@ -107,11 +107,11 @@ struct GaussGeom {
   static constexpr int OL = 32 - 2 * HALO;                // output lanes
 };
 
-// Row queue in shared memory. Each lane copies its 8 samples of source row
-// j + kQD into slot (j + kQD) % kQD with cp.async while row j is computed, so
-// kQD rows per lane are in flight without a register queue to rotate. Lanes
-// outside the row store the fill into the slot directly. Slots are
-// lane-private: no barriers.
+// Row queue of the morphology strips in shared memory. Each lane copies its 8
+// samples of source row j + QD into slot (j + QD) % QD with cp.async while
+// row j is computed, so QD rows per lane are in flight without a register
+// queue to rotate. Lanes outside the row store the fill into the slot
+// directly. Slots are lane-private: no barriers. kQD: the least depth.
 constexpr int kQD = 8;
 
 __device__ __forceinline__ void cp_async8(uint32_t saddr, const void *g) {
@@ -129,16 +129,6 @@ __device__ __forceinline__ uint2 ld_shared8(uint32_t saddr) {
   uint2 v;
   asm volatile("ld.shared.v2.u32 {%0, %1}, [%2];\n" : "=r"(v.x), "=r"(v.y) : "r"(saddr));
   return v;
-}
-
-struct RowQueue {
-  uint32_t base;  // shared address of this lane's bytes in slot 0
-  __device__ __forceinline__ uint32_t slot(int j) const { return base + (uint32_t)((j & (kQD - 1)) * 32 * kSPL); }
-};
-
-__device__ __forceinline__ RowQueue row_queue(int lane) {
-  __shared__ __align__(16) uint2 s_q[kWarpsPerBlock][kQD][32];
-  return RowQueue{(uint32_t)__cvta_generic_to_shared(&s_q[(threadIdx.x >> 5) % kWarpsPerBlock][0][lane])};
 }
 
 // A predicated copy of the lane's 8 samples at g, or the fill stored into
@@ -564,7 +554,10 @@ __device__ __forceinline__ void band_apply(const uint32_t (&h)[PR::KH][4], uint3
 // through the shared-memory row queue. The last KH rows of each pass's input
 // stay in a register ring (row t in slot t mod KH; the row loop is unrolled
 // by KH, so every slot index is a compile-time constant and nothing moves),
-// and each output row is the band decomposition of its KH input rows.
+// and each output row is the band decomposition of its KH input rows. The
+// row queue is QD = KH1 * m slots deep (at least 8), so a group of KH1 rows
+// never wraps inside it and every slot address in the unrolled group is a
+// constant offset from the group's first slot.
 template <class P1, class P2, int CN, int RH, bool MAX1, bool FUSED>
 struct MorphStrip {
   static constexpr int M1 = P1::maxd(), M2 = FUSED ? P2::maxd() : 0;
@@ -578,6 +571,13 @@ struct MorphStrip {
   static constexpr uint32_t I1 = MAX1 ? 0u : 0xFFFFFFFFu;
   static constexpr uint32_t I1p = MAX1 ? 0u : 0x00FF00FFu;
   static constexpr uint32_t I2p = MAX2 ? 0u : 0x00FF00FFu;
+  static constexpr int QD = KH1 * ((kQD + KH1 - 1) / KH1);
+  static constexpr uint32_t kSlot = 32 * kSPL;  // bytes of one queue slot
+  // Source rows that only fill the rings before the first output row, and
+  // the rows of the first steady group that compute an output before it
+  // (their stores are predicated off).
+  static constexpr int W = (KH1 - 1) + (FUSED ? KH2 - 1 : 0);
+  static constexpr int G = W > KH1 ? W - KH1 : 0;
   // Tile modes: every lane inside the row; or lanes inside, entirely
   // outside (predicated fills) or straddling the row's end with an 8-byte
   // copy into the row padding (masked per pair: the plan hands the strips
@@ -588,13 +588,16 @@ struct MorphStrip {
   long long n, gs;
   int H, first, nsrc, ylim;
   bool out_lane, live, inside;
-  RowQueue q;
-  // kInside / kEdge: the next source row to fetch and the next output row,
-  // as running pointers at this lane's samples (advanced by a stride per
-  // row; rows outside [jlo, jhi) are fills and their pointers are not read).
+  uint32_t q0, qs;  // shared address of this lane's slot 0; of the current group's first slot
+  // The next source row to fetch and the next output row, as running
+  // pointers at this lane's samples (advanced by a stride per row; rows
+  // outside [jlo, jhi) are fills and their pointers are not read). oc counts
+  // output rows from y0 (negative for the predicated-off rows before it),
+  // stored while oc < olim (0 for halo lanes and lanes past the row).
   const uint8_t *fp;
   uint8_t *op;
-  int jlo, jhi, yout;
+  int jlo, jhi, oc;
+  unsigned olim;
   uint32_t keep[4];     // kEdge: 16-bit lanes of samples inside the row
   uint32_t h1[KH1][4];  // the first pass's input rows
   uint32_t h2[KH2][4];  // the second pass's input rows (first-pass results)
@@ -611,52 +614,58 @@ struct MorphStrip {
     nsrc = min(NSRC, ylim - y0 + KH1 + KH2 - 2);
     out_lane = lane >= HALO && lane < 32 - HALO && gs < n;
     live = gs < n && gs + kSPL > 0;
-    q = row_queue(lane);
+    __shared__ __align__(16) uint2 s_q[kWarpsPerBlock][QD][32];
+    q0 = (uint32_t)__cvta_generic_to_shared(&s_q[(threadIdx.x >> 5) % kWarpsPerBlock][0][lane]);
     jlo = max(0, -first);
     jhi = max(jlo, min(nsrc, H - first));
     if (!live) jhi = jlo;  // kEdge: lanes without samples in the row only fill
     fp = s.p + (long long)first * s.stride + gs;
-    yout = y0;
-    op = d.p + (long long)y0 * d.stride + gs;
+    oc = -G;
+    olim = out_lane ? (unsigned)(ylim - y0) : 0u;
+    op = reinterpret_cast<uint8_t *>(reinterpret_cast<uintptr_t>(d.p) +
+                                     (uintptr_t)((long long)(y0 - G) * d.stride + gs));
+#pragma unroll
+    for (int r = 0; r < KH2; r++)
+#pragma unroll
+      for (int p = 0; p < 4; p++) h2[r][p] = I2p;
   }
 
-  // Source row j into its slot (rows outside [jlo, jhi): the fill). Rows
-  // are fetched in order, one per call.
-  template <int MODE>
-  __device__ __forceinline__ void fetch(int j) {
-    fetch8_inside(q.slot(j), fp, (unsigned)(j - jlo) < (unsigned)(jhi - jlo), I1);
+  // Source row j into the slot at address a (rows outside [jlo, jhi): the
+  // fill). Rows are fetched in order, one per call.
+  __device__ __forceinline__ void fetch(uint32_t a, int j) {
+    fetch8_inside(a, fp, (unsigned)(j - jlo) < (unsigned)(jhi - jlo), I1);
     fp += s.stride;
   }
 
-  // The next output row (rows y0, y0 + 1, ... in order, one per call),
-  // written when it belongs to the tile and the image.
-  template <int MODE>
+  // The next output row (rows y0 - G, y0 - G + 1, ... in order, one per
+  // call), written when it belongs to the tile and the image.
   __device__ __forceinline__ void put(const uint32_t (&o)[4]) {
-    st_global8_if(op, pack_pairs(o), out_lane && yout < ylim);
+    st_global8_if(op, pack_pairs(o), (unsigned)oc < olim);
     op += d.stride;
-    yout++;
+    oc++;
   }
 
-  // Source row j; PH = j mod KH1. Rows past nsrc (the last group of KH1)
-  // compute values that are not stored. WARM: j may still be inside the
-  // first rows that only fill the windows (checked per row, uniform).
+  // Source row j = (group start) + PH, PH = j mod KH1. Rows past nsrc (the
+  // last group of KH1) compute values that are not stored. WARM: the first
+  // group (j = PH), whose rows only fill the rings up to row W.
   template <int MODE, bool WARM, int PH>
   __device__ __forceinline__ void step(int j) {
-    cp_wait<kQD - 1>();  // row j has landed
-    const uint2 cur = ld_shared8(q.slot(j));
-    fetch<MODE>(j + kQD);
+    const uint32_t slot = qs + PH * kSlot;
+    cp_wait<QD - 1>();  // row j has landed
+    const uint2 cur = ld_shared8(slot);
+    fetch(slot, j + QD);
     cp_commit();
     unpack_pairs(cur, h1[PH]);
     if constexpr (MODE == kEdge) {
 #pragma unroll
       for (int p = 0; p < 4; p++) h1[PH][p] = (h1[PH][p] & keep[p]) | (I1p & ~keep[p]);
     }
-    if (WARM && j < KH1 - 1) return;
+    if constexpr (WARM && PH < KH1 - 1) return;
     uint32_t o1[4];
     band_apply<P1, CN, MAX1, (PH + 1) % KH1>(h1, o1);
     const int y1 = first + j - (KH1 - 1) + AY1;  // first-pass row completed
     if constexpr (!FUSED) {
-      put<MODE>(o1);
+      put(o1);
     } else {
       // First-pass row t2 = j - (KH1 - 1) goes to slot t2 mod KH2; values
       // outside the image are the second pass's identity.
@@ -667,10 +676,10 @@ struct MorphStrip {
         const uint32_t v = rin ? o1[p] : I2p;
         h2[S2][p] = MODE == kEdge ? (v & keep[p]) | (I2p & ~keep[p]) : v;
       }
-      if (WARM && j < (KH1 - 1) + (KH2 - 1)) return;
+      if constexpr (WARM && PH < W) return;
       uint32_t o2[4];
       band_apply<P2, CN, MAX2, (PH + 2) % KH2>(h2, o2);
-      put<MODE>(o2);
+      put(o2);
     }
   }
 
@@ -689,12 +698,19 @@ struct MorphStrip {
       }
     }
 #pragma unroll 1
-    for (int j = 0; j < kQD; j++) {
-      fetch<MODE>(j);
+    for (int j = 0; j < QD; j++) {
+      fetch(q0 + j * kSlot, j);
       cp_commit();
     }
+    // The first group (every tile has at least KH1 source rows), then the
+    // steady groups; the group's first slot wraps to slot 0 after QD rows.
+    qs = q0;
+    steps<MODE, true>(0, std::make_integer_sequence<int, KH1>{});
 #pragma unroll 1
-    for (int j = 0; j < nsrc; j += KH1) steps<MODE, true>(j, std::make_integer_sequence<int, KH1>{});
+    for (int j = KH1; j < nsrc; j += KH1) {
+      qs = qs == q0 + (QD - KH1) * kSlot ? q0 : qs + KH1 * kSlot;
+      steps<MODE, false>(j, std::make_integer_sequence<int, KH1>{});
+    }
   }
 
   static __device__ __forceinline__ void run(const DImg &s, const DImg &d, int tx, int ty, int lane) {
