@@ -542,7 +542,7 @@ def reference_batched(args):
 # ---------------------------------------------------------------- video-4k
 
 V_FRAMES, V_H, V_W = 300, 2160, 3840
-V_INSTANCES = 3
+V_INSTANCES = 4
 V_BYTES_PER_FRAME = V_W * V_H * 3 + V_W * V_H + 2 * V_W * V_H + 2 * V_W * V_H + 2 * 2 * V_W * V_H + 2 * V_W * V_H
 
 
@@ -1432,11 +1432,15 @@ def main():
                     help="batched-mixed: strip tile height (with --images: the full plan's 64 on a reduced plan)")
     ap.add_argument("--frames", type=int, default=0,
                     help="video-4k: N frames in HBM instead of 300 (a reduced case for profiler captures; not a bench line)")
+    ap.add_argument("--instances", type=int, default=0,
+                    help="video-4k: graph instances (and streams) taking the frames in turn (default 4)")
     args = ap.parse_args()
-    global IMAGE_LIMIT, V_FRAMES
+    global IMAGE_LIMIT, V_FRAMES, V_INSTANCES
     IMAGE_LIMIT = max(0, args.images)
     if args.frames > 0:
         V_FRAMES = args.frames
+    if args.instances > 0:
+        V_INSTANCES = args.instances
     ours, ref = WORKLOADS[args.workload]
     subs = args.workload == "batched-mixed" and not args.only and args.gpus == 1
     if args.impl == "reference":

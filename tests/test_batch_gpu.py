@@ -269,6 +269,30 @@ def test_tuning_choices_give_identical_results():
         B.tune_load(None)
 
 
+def test_warp_tile_heights_give_identical_results():
+    """One-channel u8 linear warps run tiles 32 pixels wide and 32 to 256
+    rows tall (a thread takes every 32nd row of its tile); every height gives
+    the per-call bytes, partial tiles at the bottom included."""
+    imgs = mixed_u8(6, seed=61, wmax=700, hmax=600, channels=(1,))
+    homs = [synth.perspective_params(x.shape[1], x.shape[0], seed=500 + i) for i, x in enumerate(imgs)]
+    affs = [synth.affine_params(x.shape[1], x.shape[0], seed=600 + i) for i, x in enumerate(imgs)]
+    specs = [("persp", {"m": homs, "interp": 1, "border": 0, "value": 5}),
+             ("affine", {"m": affs, "interp": 1, "border": 1, "value": 0})]
+    plan = check_plan(imgs, specs)
+    keys = sorted({s["name"] for s in plan.launch_stats()})
+    del plan
+    assert any(k.startswith("warp_perspective.u8.c1") for k in keys)
+    assert any(k.startswith("warp_affine.u8.c1") for k in keys)
+    try:
+        for rows in (32, 64, 256):
+            B.tune_load(None)
+            for k in keys:
+                B.tune_set(f"{k}.rows", rows)
+            check_plan(imgs, specs)
+    finally:
+        B.tune_load(None)
+
+
 def test_autotune_writes_a_table_the_library_reads(tmp_path):
     from visar_b200 import autotune
     imgs = mixed_u8(6, seed=51, wmax=600, hmax=400)

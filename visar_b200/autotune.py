@@ -5,9 +5,10 @@ launch per shape class. Its tuning table holds, per class key
 `<op>.<depth>.c<channels>.k<ksize>[.<element>][.<pass>].<size class>`
 (the `name` of a launch in `Batch.launch_stats()`), integer fields:
 
-  rows    tile height: rows per tile (strip ops: 8, 32 or 64 rows per warp tile;
-          row-tiled ops: rows per thread, the tile being rows x the CTA's
-          rows in flight)
+  rows    tile height: rows per tile (strip ops: 8, 32, 64 or 128 rows per
+          warp tile; one-channel u8 linear warps: 32 to 256 rows per 32-pixel
+          wide tile; row-tiled ops: rows per thread, the tile being rows x
+          the CTA's rows in flight)
   vec     samples (pixels) per thread, i.e. the vector width of the loads
           and stores: gray / threshold LUT 8 or 16 bytes, exact halving 4 or
           8 output pixels
@@ -48,8 +49,8 @@ CANDIDATES = {
     "linear": {"rows": (2, 4, 8, 16, 32), "per_sm": (2, 4, 6)},
     "morph_f": {"rows": (1, 2, 4, 8, 16), "per_sm": (2, 4)},
     "copy": {"rows": (1, 2, 4, 8, 16), "per_sm": (2, 4)},
-    "warp_affine": {"per_sm": (2, 4, 8)},
-    "warp_perspective": {"per_sm": (2, 4, 8)},
+    "warp_affine": {"rows": (32, 64, 128, 256), "per_sm": (2, 4, 8)},
+    "warp_perspective": {"rows": (32, 64, 128, 256), "per_sm": (2, 4, 8)},
 }
 FIELDS = ("rows", "vec", "per_sm")
 

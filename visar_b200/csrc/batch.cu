@@ -177,6 +177,12 @@ void row_tiles(BImg &b, long long units, int P, int rows, int h) {
   b.tiles_y = (int)ceil_div(h, (long long)rows * (256 >> lg));
 }
 
+// One-channel u8 warps with linear interpolation run OpWarp4 (4 pixels per
+// thread, tiles of 32 x L.wa.rows).
+bool warp4_class(const Launch &L) {
+  return (L.op == kOpWarpAff || L.op == kOpWarpPer) && L.depth == k8U && L.cn == 1 && L.wa.interp != 0;
+}
+
 // Tiles per image of an operation, for the launch's tuned parameters.
 void set_tiles(const Launch &L, BImg &b) {
   switch (L.op) {
@@ -210,6 +216,10 @@ void set_tiles(const Launch &L, BImg &b) {
     case kOpMorphStrip:
       b.tiles_x = (int)ceil_div((long long)b.s.w * L.cn, strip::kSPL * (32 - 2 * strip_halo(L.sub, L.cn, L.fused)));
       b.tiles_y = (int)ceil_div(b.s.h, L.rows);
+      break;
+    case kOpWarpAff: case kOpWarpPer:
+      b.tiles_x = (int)ceil_div(b.d.w, 32);
+      b.tiles_y = (int)ceil_div(b.d.h, warp4_class(L) ? L.wa.rows : 32);
       break;
     default:
       b.tiles_x = (int)ceil_div(b.d.w, 32);
@@ -300,6 +310,12 @@ void tune_and_tile(Launch &L, int num_sms) {
       }
       break;
     }
+    case kOpWarpAff: case kOpWarpPer:
+      // One-channel u8 linear warps (OpWarp4): tiles of 32 x 32..256 rows.
+      L.rows = 8;
+      L.wa.rows = tuned == 32 || tuned == 64 || tuned == 128 || tuned == 256 ? tuned : OpWarp4<true>::kDefaultRows;
+      retile();
+      break;
     default:
       L.rows = 8;
       retile();
@@ -711,7 +727,7 @@ int build_stage(Builder &B, const visar_stage &st, const std::vector<Buf> &cur, 
         b.cv = im.depth == k8U ? wp::sat_value_host<uint8_t>(value) : wp::sat_value_host<float>(value);
         b.wide = ((uintptr_t)im.v.p % 8 == 0) && (im.v.stride % 8 == 0);
         Launch *l = class_of(ls, persp ? kOpWarpPer : kOpWarpAff, im.depth, im.v.cn, 0, false);
-        l->wa = WarpArgs{interp, border};
+        l->wa = WarpArgs{interp, border, 32};
         add_img(l, b, im.input);
         u8_bytes(*l, im.v, next[i].v, depth_size(im.depth));
       }
@@ -806,7 +822,7 @@ cudaError_t run_morph(const Plan &P, const Launch &L, cudaStream_t st) {
 template <class T, bool PERSP>
 cudaError_t run_warp(const Plan &P, const Launch &L, cudaStream_t st) {
   // Pool destinations are pitched (4-byte aligned rows).
-  if (sizeof(T) == 1 && L.cn == 1 && L.wa.interp != 0) return run_op<OpWarp4<PERSP>>(P, L, L.wa, st);
+  if (warp4_class(L)) return run_op<OpWarp4<PERSP>>(P, L, L.wa, st);
   switch (L.cn) {
     case 1: return run_op<OpWarp<T, 1, PERSP>>(P, L, L.wa, st);
     case 3: return run_op<OpWarp<T, 3, PERSP>>(P, L, L.wa, st);

@@ -734,6 +734,7 @@ struct OpMorphStrip {
 
 struct WarpArgs {
   int interp, border;
+  int rows;  // OpWarp4: tile height (a multiple of 32)
 };
 
 // warpAffine / warpPerspective on 32 x 32 output tiles; a warp covers 8 x 4
@@ -782,15 +783,16 @@ struct OpWarp {
 // 32 x 4 pixels.
 template <bool PERSP>
 struct OpWarp4 {
-  static constexpr int kThreads = 256, TS = 32, kMinBlocks = 3;  // <= 85 registers (no spills)
+  // Tiles of 32 x a.rows output pixels; a thread takes 4 consecutive pixels
+  // in every 32nd row of its tile, so the tile's setup (queue ticket, image
+  // record, matrix) is paid once per 4 x rows / 32 pixels.
+  static constexpr int kThreads = 256, TS = 32, kDefaultRows = 128, kMinBlocks = 3;  // <= 85 registers (no spills)
   using Args = WarpArgs;
   static size_t smem(const Args &) { return 0; }
-  static int tiles_x(int w) { return (int)ceil_div(w, TS); }
-  static int tiles_y(int h) { return (int)ceil_div(h, TS); }
   static __device__ __forceinline__ void tile(const BImg &im, const Args &a, int tx, int ty, unsigned char *) {
-    const int y = ty * TS + (int)(threadIdx.x >> 3);
     const int x0 = tx * TS + (int)(threadIdx.x & 7) * 4;
-    if (y >= im.d.h || x0 >= im.d.w) return;
+    const int y0 = ty * a.rows, y1 = min(y0 + a.rows, im.d.h);
+    if (x0 >= im.d.w) return;
     wp::PerArgs pa{};
     wp::AffArgs aa{};
     if constexpr (PERSP) {
@@ -806,7 +808,9 @@ struct OpWarp4 {
       aa.border = a.border;
       aa.cv = im.cv;
     }
-    wp::warp4_u8<PERSP>(im.s, im.d, pa, aa, im.wide, x0, y);
+#pragma unroll 1
+    for (int y = y0 + (int)(threadIdx.x >> 3); y < y1; y += kThreads / 8)
+      wp::warp4_u8<PERSP>(im.s, im.d, pa, aa, im.wide, x0, y);
   }
 };
 
