@@ -19,9 +19,10 @@
 //    native instructions (byte-lane min/max are not). Out-of-image pixels hold
 //    the identity (morph.zig:489-519).
 //
-// Rows stream through a per-lane queue in shared memory: the copy of row
-// j + kQD (cp.async) is issued when row j is computed, so kQD rows per lane
-// are always in flight. State that moves down with the rows (the Gaussian
+// Rows stream through a per-lane queue in shared memory: the copy of a row
+// a queue depth ahead (cp.async) is issued when row j is computed, so that
+// many rows per lane are in flight (the Gaussian: 15 of 16 slots; the
+// morphology: a multiple of the element height, at least 8). State that moves down with the rows (the Gaussian
 // cascade, the morphology row windows) alternates between register sets or
 // rotates through compile-time ring slots across an unrolled row loop
 // instead of being moved.
